@@ -1,0 +1,209 @@
+/*
+ * stokesflow_b200.h -- C ABI of libstokesflow_b200.so, the B200 (sm_100a)
+ * implementation of the per-timestep hot path of StokesFlow.jl:
+ * marker->grid deposit, pseudo-transient Stokes solve, RK4 marker advection
+ * and marker->cell rebinning, on a single domain (one GPU, no MPI).
+ *
+ * Conventions
+ *  - Grid arrays are the reference's Julia arrays: dense, column-major
+ *    (x index fastest) Float64 device buffers; an (nx, ny) array A holds
+ *    A[ix, iy] (1-based) at A[(ix-1) + (iy-1)*nx].  Marker arrays are 1-D.
+ *  - All array arguments are DEVICE pointers (cudaMalloc'd, managed, or
+ *    Julia CuArray storage) unless the name ends in _host.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default).
+ *    Calls are asynchronous on that stream unless a host-side scalar result is
+ *    returned (sf_solve_stokes, sf_get_warnings, sf_stokes_residual_scale),
+ *    which synchronises the stream.
+ *  - Every function returns an sf_status (0 = SF_OK).  Warnings that the
+ *    reference prints and continues past are counted on the device instead and
+ *    read with sf_get_warnings.
+ *  - A context owns all scratch device memory for one device; it is not
+ *    thread-safe: use one context per host thread / stream.
+ *  - The reference's MPI communicator / ImplicitGlobalGrid arguments (`comm`,
+ *    `grid`) have no counterpart: the domain is a single rank, so every
+ *    overlap sum, halo update and Allreduce is the identity.
+ */
+#ifndef STOKESFLOW_B200_H
+#define STOKESFLOW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    SF_OK = 0,
+    SF_ERR_INVALID_ARG = 1,   /* bad size / NULL pointer / misaligned layout; reference: AssertionError */
+    SF_ERR_CUDA = 2,          /* a CUDA runtime call failed (message in sf_last_error)                 */
+    SF_ERR_OOM = 3,           /* scratch allocation failed                                              */
+    SF_ERR_NO_DEVICE = 4,     /* no CUDA device / device index out of range                             */
+    SF_ERR_NONFINITE = 5,     /* the PT iteration produced NaN/Inf (err is not finite)                  */
+    SF_ERR_TOO_LARGE = 6      /* a size exceeds what the entry point supports                           */
+} sf_status;
+
+typedef struct sf_ctx sf_ctx;
+
+/* ---------------------------------------------------------------------- */
+/* library / context                                                       */
+/* ---------------------------------------------------------------------- */
+int sf_version(void);                          /* (major<<16)|(minor<<8)|patch */
+const char* sf_status_string(int status);
+const char* sf_last_error(void);               /* thread-local text of the last failure */
+
+int sf_ctx_create(int device, sf_ctx** out);
+int sf_ctx_destroy(sf_ctx* ctx);
+/* Bytes of device scratch currently held by the context. */
+int sf_ctx_scratch_bytes(sf_ctx* ctx, int64_t* bytes);
+/* Number of kernels launched through the context since its creation. */
+int sf_ctx_launch_count(sf_ctx* ctx, int64_t* launches);
+
+/* Device-side counters of the reference's printed warnings.  reset != 0
+ * zeroes them after reading.  Synchronises the context's device. */
+typedef struct {
+    int64_t bad_markers;      /* MarkerToGrid.jl:66-67,120-121 "erroneous marker position"     */
+    int64_t empty_nodes;      /* MarkerToGrid.jl:166-169 "no markers close enough" (value kept) */
+    int64_t interp_failsafe;  /* MoveMarkers.jl:80-99,128-147 index-range failsafes             */
+    int64_t markers_outside;  /* sf_rebin_markers: markers outside every cell                   */
+} sf_warnings;
+int sf_get_warnings(sf_ctx* ctx, sf_warnings* out, int reset);
+
+/* ---------------------------------------------------------------------- */
+/* marker->grid deposit                                                     */
+/* ---------------------------------------------------------------------- */
+/* Replaces bilinearMarkerToGrid!(x_grid_min, y_grid_min, val_grid, x_m, y_m,
+ * val_m, dx, dy, val_wt_sum, wt_sum, grid)  (scripts/MarkerToGrid.jl:18-38).
+ * val_grid is (nx, ny).  Each node gets sum(w*val)/sum(w) over the markers of
+ * its four adjacent cells, with the bilinear weights of MarkerToGrid.jl:110-155;
+ * the sums are taken in ascending marker index, the order of the reference's
+ * serial CPU loop, so the result is bit-identical to it and deterministic
+ * (no floating-point atomics).  Nodes with zero weight keep their previous
+ * value (safeDivision, :164-172) and are counted in empty_nodes; markers whose
+ * cell is outside 0..nx x 0..ny are skipped and counted in bad_markers.
+ * val_wt_sum / wt_sum are optional (NULL): when given they are the
+ * reference's work arrays of n_sum elements with leading dimension ld_sum
+ * (ld_sum >= nx), zeroed and then filled with the sums as in :24-28. */
+int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min,
+                               double* val_grid, int64_t nx, int64_t ny,
+                               const double* x_m, const double* y_m, const double* val_m,
+                               int64_t nm, double dx, double dy,
+                               double* val_wt_sum, double* wt_sum, int64_t ld_sum, int64_t n_sum,
+                               void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* pseudo-transient Stokes solve                                             */
+/* ---------------------------------------------------------------------- */
+typedef struct {
+    double dt;               /* compute_dt of the final velocities (StokesSolver_multixpu.jl:95)      */
+    double T_eff;            /* GB/s, reference definition 6*Nx*Ny*8 B / t_it (:78-81)                */
+    double runtime;          /* seconds of iterations >= 11 (:38,44-46,78), CUDA-event timed          */
+    int64_t iters;           /* niter                                                                 */
+    double err;              /* last residual norm max(mean|Rx|, mean|Ry|, mean|divV|) (2*eps if none)*/
+    int64_t n_checks;        /* residual checks performed (every ncheck iterations)                   */
+    int32_t converged;       /* err <= eps                                                             */
+    int32_t reserved;
+    double loop_ms;          /* device time of the whole iteration loop                                */
+    double bytes_per_iter;   /* essential HBM bytes of one fused PT iteration (see DESIGN)             */
+    double T_eff_essential;  /* bytes_per_iter * iters / loop time, GB/s                               */
+    int64_t fused_launches;  /* launches of the fused PT iteration kernel                              */
+    double fused_ms;         /* device time of the fused launches alone (0 unless timing requested)    */
+} sf_solve_info;
+
+/* Replaces solveStokes!(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy,
+ * divV, dtPt, Rx, Ry, dVxdt, dVydt, dtVx, dtVy, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny,
+ * dt, maxdisp, comm; use_free_surface_stabilization, eps, print_info, iterMax)
+ * (scripts/StokesSolver_multixpu.jl:14-96).  Sizes as in the reference:
+ *   P (Nx-1,Ny-1) Vx_pad (Nx+2,Ny+1) Vy_pad (Nx+1,Ny+2) rho_vy (Nx+1,Ny) mu_b (Nx,Ny)
+ *   mu_p,txx,tyy,divV,dtPt (Nx-1,Ny-1) txy (Nx,Ny) Rx,dVxdt,dtVx (Nx-2,Ny-1)
+ *   Ry,dVydt,dtVy (Nx-1,Ny-2) Vx_s (Nx,Ny+1) Vy_s (Nx+1,Ny).
+ * State (P, Vx_s, Vy_s, dVxdt, dVydt) is read as the warm start and written
+ * back; Vx_pad / Vy_pad receive the padded, mirrored velocities.  The work
+ * arrays txx, tyy, txy, divV, dtPt, Rx, Ry, dtVx, dtVy may be NULL; when given
+ * they end with the values the reference leaves in them.  Synchronises the
+ * stream (the stopping test needs the residual on the host).  `info` may be
+ * NULL.  Returns SF_ERR_NONFINITE if the residual becomes NaN/Inf. */
+int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad,
+                    const double* rho_vy, const double* mu_b, const double* mu_p,
+                    double* txx, double* tyy, double* txy, double* divV, double* dtPt,
+                    double* Rx, double* Ry, double* dVxdt, double* dVydt, double* dtVx,
+                    double* dtVy, double* Vx_s, double* Vy_s, double g_y, double dx, double dy,
+                    int64_t Nx, int64_t Ny, double dt, double maxdisp,
+                    int use_free_surface_stabilization, double eps, int print_info,
+                    int64_t iter_max, void* stream, sf_solve_info* info);
+
+/* Scale for a relative stopping test: mean(|g_y * rho_vy|) over the interior
+ * region of Ry (rho_vy[2:Nx, 2:Ny-1]), i.e. the residual norm of V = P = 0.
+ * A relative tolerance rtol is the absolute eps = rtol * scale.  (No reference
+ * counterpart: the reference only has the absolute eps.) */
+int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int64_t Ny,
+                             double g_y, void* stream, double* scale);
+
+/* ---------------------------------------------------------------------- */
+/* RK4 marker advection and rebinning                                        */
+/* ---------------------------------------------------------------------- */
+/* Replaces moveMarkersRK4!(x_m, y_m, Vx, Vy, x_vx_min, y_vx_min, x_vy_min,
+ * y_vy_min, dt, lx, ly, dx, dy)  (scripts/MoveMarkers.jl:15-69): classical RK4
+ * with the continuity-based velocity interpolation of interpolateV
+ * (:76-174) on the padded Vx (vx_nx, vx_ny) and Vy (vy_nx, vy_ny), positions
+ * clamped to [0,lx] x [0,ly].  Same operation order as the reference: the
+ * result is bit-identical to it.  Failsafe index clamps are counted. */
+int sf_move_markers_rk4(sf_ctx* ctx, double* x_m, double* y_m, int64_t nm,
+                        const double* Vx, int64_t vx_nx, int64_t vx_ny,
+                        const double* Vy, int64_t vy_nx, int64_t vy_ny,
+                        double x_vx_min, double y_vx_min, double x_vy_min, double y_vy_min,
+                        double dt, double lx, double ly, double dx, double dy, void* stream);
+
+/* Marker->cell rebinning: a stable counting sort of the markers by the cell
+ * topleftIndexRelDist (scripts/common.jl:22-33) gives them on a grid of nx x ny
+ * nodes, cells keyed (ix, iy) in 0..nx x 0..ny -> key ix + iy*(nx+1).
+ * counts[(nx+1)*(ny+1)] receives the markers per cell, offsets[(nx+1)*(ny+1)+1]
+ * the exclusive prefix sum, perm[nm] the marker indices (0-based) in cell
+ * order, ascending within a cell.  Markers outside every cell are left out of
+ * perm (perm is then shorter: offsets[last] markers) and counted in
+ * markers_outside.  counts / offsets / perm may each be NULL.  The reference
+ * never reorders a rank's markers (exchangeMarkers, MarkerExchange.jl:8-163,
+ * is the identity on one rank), so neither does this: x_m / y_m are not moved. */
+int sf_rebin_markers(sf_ctx* ctx, const double* x_m, const double* y_m, int64_t nm,
+                     double x_grid_min, double y_grid_min, double dx, double dy,
+                     int64_t nx, int64_t ny, int32_t* counts, int32_t* offsets, int32_t* perm,
+                     void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* marker initialisation (scripts/common.jl:40-110, single rank)             */
+/* ---------------------------------------------------------------------- */
+/* Number of markers initializeMarkersCPU places on one rank. */
+int sf_marker_count(int64_t marker_density, int64_t nx, int64_t ny, int64_t* nmx, int64_t* nmy);
+
+/* initializeMarkersCPU (common.jl:40-90) on one rank: LinRange sub-grid
+ * (x outer, y inner) plus jitter x += (u - 0.5)*jitter*dxm, u from the
+ * counter-based generator sf_uniform(seed, 2m) / (seed, 2m+1).  jitter = 1 is
+ * the reference's +-0.5 sub-spacing; jitter = 0 is RAND_MARKER_POS = false.
+ * _host works on host memory, the other on device memory. */
+int sf_init_markers_host(int64_t marker_density, double lx, double ly, double dx, double dy,
+                         int64_t nx, int64_t ny, double jitter, uint64_t seed,
+                         double* x_m_host, double* y_m_host);
+int sf_init_markers(sf_ctx* ctx, int64_t marker_density, double lx, double ly, double dx, double dy,
+                    int64_t nx, int64_t ny, double jitter, uint64_t seed,
+                    double* x_m, double* y_m, void* stream);
+double sf_uniform(uint64_t seed, uint64_t counter);
+
+/* setInitialMarkerProperties! (common.jl:104-110) for the layered
+ * air / plume / matrix model of StokesFlow2D_multixpu.jl:382-404:
+ * y < air_height -> air, else (x-px)^2+(y-py)^2 < r^2 -> plume, else matrix. */
+typedef struct {
+    double air_height;
+    double plume_x, plume_y, plume_r;
+    double rho_air, rho_matrix, rho_plume;
+    double mu_air, mu_matrix, mu_plume;
+} sf_plume_model;
+int sf_set_marker_properties_host(const sf_plume_model* model, const double* x_m_host,
+                                  const double* y_m_host, int64_t nm, double x0, double y0,
+                                  double* rho_m_host, double* mu_m_host);
+int sf_set_marker_properties(sf_ctx* ctx, const sf_plume_model* model, const double* x_m,
+                             const double* y_m, int64_t nm, double x0, double y0,
+                             double* rho_m, double* mu_m, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STOKESFLOW_B200_H */

@@ -1,0 +1,387 @@
+// sf_core.cu -- context, errors, scratch, prefix scan, warning counters and
+// marker initialisation (scripts/common.jl:40-110) for libstokesflow_b200.so.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_last_error = buf;
+    if (e == cudaErrorMemoryAllocation) return SF_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInvalidDevice || e == cudaErrorInsufficientDriver)
+        return SF_ERR_NO_DEVICE;
+    return SF_ERR_CUDA;
+}
+
+int set_device(sf_ctx* ctx) {
+    SF_CUDA(cudaSetDevice(ctx->device));
+    return SF_OK;
+}
+
+int ensure(sf_ctx* ctx, Scratch& s, size_t bytes) {
+    if (bytes <= s.bytes) return SF_OK;
+    (void)ctx;
+    if (s.ptr) {
+        SF_CUDA(cudaFree(s.ptr));
+        s.ptr = nullptr;
+        s.bytes = 0;
+    }
+    size_t want = (size_t)round_up((int64_t)bytes, 1 << 20);
+    cudaError_t e = cudaMalloc(&s.ptr, want);
+    if (e != cudaSuccess) {
+        s.ptr = nullptr;
+        (void)cudaGetLastError();
+        return cuda_fail(e, "cudaMalloc(scratch)", __FILE__, __LINE__);
+    }
+    s.bytes = want;
+    return SF_OK;
+}
+
+// --------------------------------------------------------------------------
+// exclusive scan of int32 (3 passes: tile sums, scan of tile sums, tile scan)
+// --------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ int32_t block_exclusive_scan(int32_t v, int32_t* warp_sums, int32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0;
+        int32_t s = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sums[lane] = s - w;  // exclusive warp offsets
+        if (lane == 31) *total = s;
+    }
+    __syncthreads();
+    int32_t r = warp_sums[warp] + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_tile_sums(const int32_t* __restrict__ in, int64_t n, int32_t* __restrict__ tile_sums) {
+    __shared__ int32_t warp_sums[32];
+    __shared__ int32_t total;
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k)
+        if (base + k < n) s += in[base + k];
+    block_exclusive_scan(s, warp_sums, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// single block: exclusive scan of the tile sums in place, grand total -> *d_total
+__global__ void k_scan_tile_offsets(int32_t* __restrict__ tile_sums, int64_t ntiles, int32_t* __restrict__ d_total) {
+    __shared__ int32_t warp_sums[32];
+    __shared__ int32_t total;
+    int32_t carry = 0;
+    for (int64_t b0 = 0; b0 < ntiles; b0 += SCAN_THREADS) {
+        int64_t i = b0 + threadIdx.x;
+        int32_t v = (i < ntiles) ? tile_sums[i] : 0;
+        int32_t e = block_exclusive_scan(v, warp_sums, &total);
+        if (i < ntiles) tile_sums[i] = carry + e;
+        carry += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && d_total) *d_total = carry;
+}
+
+__global__ void k_scan_tiles(const int32_t* in, int32_t* out, int64_t n, const int32_t* __restrict__ tile_offsets) {
+    __shared__ int32_t warp_sums[32];
+    __shared__ int32_t total;
+    int64_t base = (int64_t)blockIdx.x * SCAN_TILE + (int64_t)threadIdx.x * SCAN_ITEMS;
+    int32_t v[SCAN_ITEMS];
+    int32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int32_t e = block_exclusive_scan(s, warp_sums, &total) + tile_offsets[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; ++k) {
+        if (base + k < n) out[base + k] = e;
+        e += v[k];
+    }
+}
+
+int exclusive_scan_i32(sf_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* d_total,
+                       cudaStream_t stream) {
+    int64_t ntiles = ceil_div(n, SCAN_TILE);
+    if (ntiles == 0) {
+        if (d_total) SF_CUDA(cudaMemsetAsync(d_total, 0, sizeof(int32_t), stream));
+        return SF_OK;
+    }
+    int rc = ensure(ctx, ctx->scan_tmp, (size_t)ntiles * sizeof(int32_t));
+    if (rc) return rc;
+    int32_t* tiles = (int32_t*)ctx->scan_tmp.ptr;
+    k_scan_tile_sums<<<(unsigned)ntiles, SCAN_THREADS, 0, stream>>>(in, n, tiles);
+    SF_LAUNCHED(ctx);
+    k_scan_tile_offsets<<<1, SCAN_THREADS, 0, stream>>>(tiles, ntiles, d_total);
+    SF_LAUNCHED(ctx);
+    k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, stream>>>(in, out, n, tiles);
+    SF_LAUNCHED(ctx);
+    return SF_OK;
+}
+
+// --------------------------------------------------------------------------
+// marker initialisation, scripts/common.jl:40-110 (single rank)
+// --------------------------------------------------------------------------
+struct MarkerLayout {
+    double xlimlo, xlimhi, ylimlo, ylimhi, dxm, dym;
+    int64_t nmx, nmy;
+};
+
+static MarkerLayout marker_layout(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny) {
+    MarkerLayout L;
+    L.dxm = dx / (double)md;
+    L.dym = dy / (double)md;
+    // one rank: every side is a physical boundary (common.jl:54-57,65-68)
+    L.xlimlo = L.dxm / 2.0;
+    L.xlimhi = lx - L.dxm / 2.0;
+    L.ylimlo = L.dym / 2.0;
+    L.ylimhi = ly - L.dym / 2.0;
+    L.nmx = md * (nx - 1);   // common.jl:73-74
+    L.nmy = md * (ny - 1);
+    return L;
+}
+
+// Julia LinRange(a, b, n)[k] (1-based k): lerpi(k-1, n-1, a, b) = fma(t, b, fma(-t, a, a))
+__host__ __device__ __forceinline__ double linrange_at(double a, double b, int64_t n, int64_t k) {
+    if (n == 1) return a;
+    double t = (double)(k - 1) / (double)(n - 1);
+    return fma(t, b, fma(-t, a, a));
+}
+
+__host__ __device__ __forceinline__ void marker_position(const MarkerLayout& L, double jitter, uint64_t seed,
+                                                         int64_t m, double* x, double* y) {
+    int64_t ix = m / L.nmy + 1, iy = m % L.nmy + 1;  // x outer, y inner (common.jl:85-91)
+    double xv = linrange_at(L.xlimlo, L.xlimhi, L.nmx, ix);
+    double yv = linrange_at(L.ylimlo, L.ylimhi, L.nmy, iy);
+    if (jitter != 0.0) {
+        double ux = uniform01(seed, (uint64_t)(2 * m));
+        double uy = uniform01(seed, (uint64_t)(2 * m + 1));
+        // x .+= (u - 0.5) * jitter * dxm, two roundings per product (no contraction)
+        xv = xv + (ux - 0.5) * jitter * L.dxm;
+        yv = yv + (uy - 0.5) * jitter * L.dym;
+    }
+    *x = xv;
+    *y = yv;
+}
+
+__global__ void k_init_markers(MarkerLayout L, double jitter, uint64_t seed, double* __restrict__ x,
+                               double* __restrict__ y) {
+    int64_t nm = L.nmx * L.nmy;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm; m += (int64_t)gridDim.x * blockDim.x)
+        marker_position(L, jitter, seed, m, &x[m], &y[m]);
+}
+
+// StokesFlow2D_multixpu.jl:387-404 density / viscosity closures
+__host__ __device__ __forceinline__ double plume_eval(const sf_plume_model& M, double x, double y, double air,
+                                                      double mat, double pl) {
+    if (y < M.air_height) return air;
+    double ddx = x - M.plume_x, ddy = y - M.plume_y;
+    if (ddx * ddx + ddy * ddy < M.plume_r * M.plume_r) return pl;
+    return mat;
+}
+
+__global__ void k_set_props(sf_plume_model M, const double* __restrict__ x, const double* __restrict__ y,
+                            int64_t nm, double x0, double y0, double* __restrict__ rho, double* __restrict__ mu) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nm; m += (int64_t)gridDim.x * blockDim.x) {
+        double xx = x0 + x[m], yy = y0 + y[m];
+        rho[m] = plume_eval(M, xx, yy, M.rho_air, M.rho_matrix, M.rho_plume);
+        mu[m] = plume_eval(M, xx, yy, M.mu_air, M.mu_matrix, M.mu_plume);
+    }
+}
+
+}  // namespace sf
+
+using namespace sf;
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+int sf_version(void) { return (0 << 16) | (1 << 8) | 0; }
+
+const char* sf_status_string(int status) {
+    switch (status) {
+        case SF_OK: return "ok";
+        case SF_ERR_INVALID_ARG: return "invalid argument";
+        case SF_ERR_CUDA: return "CUDA error";
+        case SF_ERR_OOM: return "out of device memory";
+        case SF_ERR_NO_DEVICE: return "no CUDA device";
+        case SF_ERR_NONFINITE: return "non-finite residual";
+        case SF_ERR_TOO_LARGE: return "size exceeds the supported maximum";
+        default: return "unknown status";
+    }
+}
+
+const char* sf_last_error(void) { return g_last_error.c_str(); }
+
+int sf_ctx_create(int device, sf_ctx** out) {
+    if (!out) return fail(SF_ERR_INVALID_ARG, "sf_ctx_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        (void)cudaGetLastError();
+        return fail(SF_ERR_NO_DEVICE, "sf_ctx_create: no CUDA device");
+    }
+    if (device < 0 || device >= n) return fail(SF_ERR_NO_DEVICE, "sf_ctx_create: device index out of range");
+    sf_ctx* c = new sf_ctx();
+    c->device = device;
+    int rc = set_device(c);
+    if (rc) { delete c; return rc; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
+    if (cudaMalloc(&c->d_counters, sizeof(unsigned long long) * CNT_N) != cudaSuccess ||
+        cudaMalloc(&c->d_scalars, sizeof(double) * SC_N) != cudaSuccess ||
+        cudaMallocHost(&c->h_scalars, sizeof(double) * SC_N) != cudaSuccess ||
+        cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess ||
+        cudaEventCreate(&c->ev_c) != cudaSuccess || cudaEventCreate(&c->ev_d) != cudaSuccess) {
+        cudaError_t le = cudaGetLastError();
+        sf_ctx_destroy(c);
+        return cuda_fail(le, "sf_ctx_create allocation", __FILE__, __LINE__);
+    }
+    cudaMemset(c->d_counters, 0, sizeof(unsigned long long) * CNT_N);
+    cudaMemset(c->d_scalars, 0, sizeof(double) * SC_N);
+    SF_CUDA(cudaDeviceSynchronize());
+    *out = c;
+    return SF_OK;
+}
+
+int sf_ctx_destroy(sf_ctx* c) {
+    if (!c) return SF_OK;
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
+    Scratch* all[] = {&c->keys, &c->counts, &c->offsets, &c->cursor, &c->perm, &c->scan_tmp, &c->fields, &c->partials};
+    for (Scratch* s : all)
+        if (s->ptr) cudaFree(s->ptr);
+    if (c->d_counters) cudaFree(c->d_counters);
+    if (c->d_scalars) cudaFree(c->d_scalars);
+    if (c->h_scalars) cudaFreeHost(c->h_scalars);
+    cudaEvent_t evs[] = {c->ev_a, c->ev_b, c->ev_c, c->ev_d};
+    for (cudaEvent_t ev : evs)
+        if (ev) cudaEventDestroy(ev);
+    delete c;
+    return SF_OK;
+}
+
+int sf_ctx_scratch_bytes(sf_ctx* c, int64_t* bytes) {
+    if (!c || !bytes) return fail(SF_ERR_INVALID_ARG, "sf_ctx_scratch_bytes: NULL argument");
+    const Scratch* all[] = {&c->keys, &c->counts, &c->offsets, &c->cursor, &c->perm, &c->scan_tmp, &c->fields, &c->partials};
+    int64_t b = 0;
+    for (const Scratch* s : all) b += (int64_t)s->bytes;
+    *bytes = b;
+    return SF_OK;
+}
+
+int sf_ctx_launch_count(sf_ctx* c, int64_t* launches) {
+    if (!c || !launches) return fail(SF_ERR_INVALID_ARG, "sf_ctx_launch_count: NULL argument");
+    *launches = c->launches;
+    return SF_OK;
+}
+
+int sf_get_warnings(sf_ctx* c, sf_warnings* out, int reset) {
+    if (!c || !out) return fail(SF_ERR_INVALID_ARG, "sf_get_warnings: NULL argument");
+    int rc = set_device(c);
+    if (rc) return rc;
+    unsigned long long h[CNT_N];
+    SF_CUDA(cudaDeviceSynchronize());
+    SF_CUDA(cudaMemcpy(h, c->d_counters, sizeof(h), cudaMemcpyDeviceToHost));
+    out->bad_markers = (int64_t)h[CNT_BAD_MARKERS];
+    out->empty_nodes = (int64_t)h[CNT_EMPTY_NODES];
+    out->interp_failsafe = (int64_t)h[CNT_INTERP_FAILSAFE];
+    out->markers_outside = (int64_t)h[CNT_OUTSIDE];
+    if (reset) SF_CUDA(cudaMemset(c->d_counters, 0, sizeof(h)));
+    return SF_OK;
+}
+
+int sf_marker_count(int64_t md, int64_t nx, int64_t ny, int64_t* nmx, int64_t* nmy) {
+    if (md < 1 || nx < 2 || ny < 2 || !nmx || !nmy) return fail(SF_ERR_INVALID_ARG, "sf_marker_count: bad arguments");
+    *nmx = md * (nx - 1);
+    *nmy = md * (ny - 1);
+    return SF_OK;
+}
+
+double sf_uniform(uint64_t seed, uint64_t counter) { return uniform01(seed, counter); }
+
+int sf_init_markers_host(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny,
+                         double jitter, uint64_t seed, double* x, double* y) {
+    if (md < 1 || nx < 2 || ny < 2 || !x || !y) return fail(SF_ERR_INVALID_ARG, "sf_init_markers_host: bad arguments");
+    MarkerLayout L = marker_layout(md, lx, ly, dx, dy, nx, ny);
+    int64_t nm = L.nmx * L.nmy;
+    for (int64_t m = 0; m < nm; ++m) marker_position(L, jitter, seed, m, &x[m], &y[m]);
+    return SF_OK;
+}
+
+int sf_init_markers(sf_ctx* c, int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny,
+                    double jitter, uint64_t seed, double* x, double* y, void* stream) {
+    if (!c || md < 1 || nx < 2 || ny < 2 || !x || !y) return fail(SF_ERR_INVALID_ARG, "sf_init_markers: bad arguments");
+    int rc = set_device(c);
+    if (rc) return rc;
+    MarkerLayout L = marker_layout(md, lx, ly, dx, dy, nx, ny);
+    int64_t nm = L.nmx * L.nmy;
+    if (nm == 0) return SF_OK;
+    unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nm, 256), (int64_t)c->num_sms * 16);
+    k_init_markers<<<blocks, 256, 0, as_stream(stream)>>>(L, jitter, seed, x, y);
+    SF_LAUNCHED(c);
+    return SF_OK;
+}
+
+int sf_set_marker_properties_host(const sf_plume_model* M, const double* x, const double* y, int64_t nm, double x0,
+                                  double y0, double* rho, double* mu) {
+    if (!M || nm < 0 || (nm > 0 && (!x || !y || !rho || !mu)))
+        return fail(SF_ERR_INVALID_ARG, "sf_set_marker_properties_host: bad arguments");
+    for (int64_t m = 0; m < nm; ++m) {
+        double xx = x0 + x[m], yy = y0 + y[m];
+        rho[m] = plume_eval(*M, xx, yy, M->rho_air, M->rho_matrix, M->rho_plume);
+        mu[m] = plume_eval(*M, xx, yy, M->mu_air, M->mu_matrix, M->mu_plume);
+    }
+    return SF_OK;
+}
+
+int sf_set_marker_properties(sf_ctx* c, const sf_plume_model* M, const double* x, const double* y, int64_t nm,
+                             double x0, double y0, double* rho, double* mu, void* stream) {
+    if (!c || !M || nm < 0 || (nm > 0 && (!x || !y || !rho || !mu)))
+        return fail(SF_ERR_INVALID_ARG, "sf_set_marker_properties: bad arguments");
+    if (nm == 0) return SF_OK;
+    int rc = set_device(c);
+    if (rc) return rc;
+    unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nm, 256), (int64_t)c->num_sms * 16);
+    k_set_props<<<blocks, 256, 0, as_stream(stream)>>>(*M, x, y, nm, x0, y0, rho, mu);
+    SF_LAUNCHED(c);
+    return SF_OK;
+}
+
+}  // extern "C"

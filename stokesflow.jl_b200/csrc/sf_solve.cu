@@ -1,0 +1,747 @@
+// sf_solve.cu -- pseudo-transient Stokes solve (scripts/StokesSolver_multixpu.jl)
+// for libstokesflow_b200.so.
+//
+// The reference runs, per PT iteration, compute_P_tau! -> compute_dV! ->
+// compute_V! -> four BC kernels (:48-57), with tau, divV, dtau* stored as full
+// arrays.  Here one fused kernel does the whole iteration:
+//
+//   * every CTA owns a BX x BY tile of points (i, j), 0 <= i < Nx-1,
+//     0 <= j < Ny-1 (the pressure index space, which contains the dVx and dVy
+//     index spaces);
+//   * it stages old Vx, Vy, rho (tile + 2 halo) and old P, mu_p, mu_b
+//     (tile + 1 halo) in shared memory, computes P_new, tau_xx, tau_yy,
+//     tau_xy on the tile + 1 halo (the halo row/column is recomputed by the
+//     neighbouring CTA, which is cheaper than a grid-wide barrier), then the
+//     residuals, the damped rates dV and the new velocities of its tile;
+//   * tau, divV, dtau* are never stored (dtau* is recomputed from mu_p);
+//   * the free-slip ghost rows / columns of the new velocities are written by
+//     the CTAs on the domain edge, in the reference's BC order (:53-56);
+//   * V and P are double-buffered (the iteration is Jacobi-like: every read is
+//     an old value), dV is updated in place.
+//
+// HBM bytes per iteration: read Vx, Vy, P, dVx, dVy, rho, mu_b, mu_p and write
+// Vx, Vy, P, dVx, dVy -- 13 arrays, ~104 * Nx * Ny bytes.
+//
+// Fields live in a padded internal layout (one leading dimension LD, a
+// multiple of 32 doubles, for every field) packed from / unpacked to the
+// caller's Julia-layout arrays once per solve.  Every iteration on the check
+// schedule additionally stores tau / divV and runs the residual + norm
+// kernels; dt updates (every ndtupdate) run a max|V| reduction whose result
+// stays on the device.  The only host synchronisation is the residual test.
+//
+// All floating-point expressions keep the reference's evaluation order and
+// the file is compiled with -fmad=false: the iterates are bit-identical to
+// the reference's (only the summation order inside the residual norm differs).
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+enum {
+    F_VXA, F_VXB, F_VYA, F_VYB, F_PA, F_PB, F_DVX, F_DVY, F_RHO, F_MUB, F_MUP,
+    F_TXX, F_TYY, F_TXY, F_DIV, F_RX, F_RY, F_NUM
+};
+
+struct Layout {
+    int64_t Nx, Ny, LD, rows, fstride;
+    double* base;
+    double* f(int k) const { return base + (int64_t)k * fstride; }
+};
+
+struct PTParams {
+    const double* __restrict__ Vx_in;
+    const double* __restrict__ Vy_in;
+    const double* __restrict__ P_in;
+    double* __restrict__ Vx_out;
+    double* __restrict__ Vy_out;
+    double* __restrict__ P_out;
+    double* __restrict__ dVx;
+    double* __restrict__ dVy;
+    const double* __restrict__ rho;
+    const double* __restrict__ mub;
+    const double* __restrict__ mup;
+    double* __restrict__ txx;
+    double* __restrict__ tyy;
+    double* __restrict__ txy;
+    double* __restrict__ divV;
+    const double* __restrict__ dt_ptr;
+    int Nx, Ny;
+    int64_t LD;
+    double _dx, _dy, g_y, dampX, dampY;
+    double c_vsc;    // Vsc * min_dxy2            (StokesSolver_multixpu.jl:129)
+    double c_ptsc;   // Ptsc * 4.1                (:131)
+    double max_nxy;  // max(nx_g(), ny_g())       (:21)
+};
+
+// ---------------------------------------------------------------------------
+// fused PT iteration
+// ---------------------------------------------------------------------------
+template <int BX, int BY, int TY, bool STORE>
+__global__ void __launch_bounds__(BX * TY) k_pt_iter(PTParams p) {
+    constexpr int W2 = BX + 2, H2 = BY + 2;  // V / rho tiles
+    constexpr int W1 = BX + 1, H1 = BY + 1;  // P / tau tiles
+    constexpr int NT = BX * TY;
+    __shared__ double sVx[H2][W2];
+    __shared__ double sVy[H2][W2];
+    __shared__ double sRho[H2][W2];
+    __shared__ double sP[H1][W1];     // old P, then new P
+    __shared__ double sMup[H1][W1];
+    __shared__ double sTxy[H1][W1];   // mu_b, then tau_xy
+    __shared__ double sTxx[H1][W1];
+    __shared__ double sTyy[H1][W1];
+
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int64_t LD = p.LD;
+
+    // ---- owned-point state into registers (issued first) ----
+    constexpr int RPT = BY / TY;  // owned rows per thread
+    double dvx_old[RPT], dvy_old[RPT];
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        int i = i0 + threadIdx.x, j = j0 + threadIdx.y + r * TY;
+        int64_t o = i + (int64_t)j * LD;
+        dvx_old[r] = (i < Nx - 2 && j < Ny - 1) ? p.dVx[o] : 0.0;
+        dvy_old[r] = (i < Nx - 1 && j < Ny - 2) ? p.dVy[o] : 0.0;
+    }
+    // ---- stage tiles ----
+    for (int idx = tid; idx < W2 * H2; idx += NT) {
+        int a = idx % W2, b = idx / W2;
+        int i = i0 + a, j = j0 + b;
+        int64_t o = i + (int64_t)j * LD;
+        sVx[b][a] = (i < Nx && j < Ny + 1) ? p.Vx_in[o] : 0.0;
+        sVy[b][a] = (i < Nx + 1 && j < Ny) ? p.Vy_in[o] : 0.0;
+        sRho[b][a] = (i < Nx + 1 && j < Ny) ? p.rho[o] : 0.0;
+    }
+    for (int idx = tid; idx < W1 * H1; idx += NT) {
+        int a = idx % W1, b = idx / W1;
+        int i = i0 + a, j = j0 + b;
+        int64_t o = i + (int64_t)j * LD;
+        bool pp = (i < Nx - 1 && j < Ny - 1);
+        sP[b][a] = pp ? p.P_in[o] : 0.0;
+        sMup[b][a] = pp ? p.mup[o] : 0.0;
+        sTxy[b][a] = (i < Nx && j < Ny) ? p.mub[o] : 0.0;
+    }
+    __syncthreads();
+
+    const double _dx = p._dx, _dy = p._dy;
+    // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
+    for (int idx = tid; idx < W1 * H1; idx += NT) {
+        int a = idx % W1, b = idx / W1;
+        int i = i0 + a, j = j0 + b;
+        if (i < Nx - 1 && j < Ny - 1) {
+            double vx1 = sVx[b + 1][a], vx2 = sVx[b + 1][a + 1];
+            double vy1 = sVy[b][a + 1], vy2 = sVy[b + 1][a + 1];
+            double dVx_dx = (vx2 - vx1) * _dx;
+            double dVy_dy = (vy2 - vy1) * _dy;
+            double div_V = dVx_dx + dVy_dy;
+            double mu = sMup[b][a];
+            double dtP = p.c_ptsc * mu / p.max_nxy;       // Ptsc*4.1*mu_p/max_nxy (:131)
+            double Pn = sP[b][a] - dtP * div_V;
+            sP[b][a] = Pn;
+            double txx = 2.0 * mu * (dVx_dx - 1.0 / 3.0 * div_V);
+            double tyy = 2.0 * mu * (dVy_dy - 1.0 / 3.0 * div_V);
+            sTxx[b][a] = txx;
+            sTyy[b][a] = tyy;
+            if (STORE && a < BX && b < BY) {
+                int64_t o = i + (int64_t)j * LD;
+                p.divV[o] = div_V;
+                p.txx[o] = txx;
+                p.tyy[o] = tyy;
+            }
+        }
+        if (i < Nx && j < Ny) {
+            double vx0 = sVx[b][a], vx1 = sVx[b + 1][a];
+            double vy0 = sVy[b][a], vy1 = sVy[b][a + 1];
+            double dVx_dy = (vx1 - vx0) * _dy;
+            double dVy_dx = (vy1 - vy0) * _dx;
+            double t = 2.0 * sTxy[b][a] * 0.5 * (dVx_dy + dVy_dx);
+            sTxy[b][a] = t;
+            if (STORE && (a < BX || i == Nx - 1) && (b < BY || j == Ny - 1)) p.txy[i + (int64_t)j * LD] = t;
+        }
+    }
+    __syncthreads();
+
+    // ---- stage 2: compute_dV! (:209-219), compute_V! (:226-234), BCs (:53-56) ----
+    const double dt = *p.dt_ptr;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int a = threadIdx.x, b = threadIdx.y + r * TY;
+        const int i = i0 + a, j = j0 + b;
+        if (i >= Nx - 1 || j >= Ny - 1) continue;
+        p.P_out[i + (int64_t)j * LD] = sP[b][a];
+        if (i < Nx - 2) {
+            // compute_ResX (:176-182)
+            double Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy
+                        - (sP[b][a + 1] - sP[b][a]) * _dx;
+            double dv = p.dampX * dvx_old[r] + Rx;
+            p.dVx[i + (int64_t)j * LD] = dv;
+            double dtau = p.c_vsc / ((sMup[b][a] + sMup[b][a + 1]) * 0.5) / 4.1;  // :129
+            double vn = sVx[b + 1][a + 1] + dtau * dv;
+            p.Vx_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
+            if (j == 0) p.Vx_out[(i + 1)] = vn;                                   // bc_y_noflux!
+            if (j == Ny - 2) p.Vx_out[(i + 1) + (int64_t)Ny * LD] = vn;
+        }
+        if (j < Ny - 2) {
+            // compute_ResY (:189-202)
+            double av_inn_y_Vx = 0.25 * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
+            double d_xi_2_rho = sRho[b + 1][a + 2] - sRho[b + 1][a];
+            double d_yi_2_rho = sRho[b + 2][a + 1] - sRho[b][a + 1];
+            double Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx
+                        - (sP[b + 1][a] - sP[b][a]) * _dy
+                        + p.g_y * (sRho[b + 1][a + 1] - dt * (av_inn_y_Vx * d_xi_2_rho * 0.5 * _dx
+                                                               + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
+            double dv = p.dampY * dvy_old[r] + Ry;
+            p.dVy[i + (int64_t)j * LD] = dv;
+            double dtau = p.c_vsc / ((sMup[b][a] + sMup[b + 1][a]) * 0.5) / 4.1;  // :130
+            double vn = sVy[b + 1][a + 1] + dtau * dv;
+            p.Vy_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
+            if (i == 0) p.Vy_out[(int64_t)(j + 1) * LD] = vn;                     // bc_x_noflux!
+            if (i == Nx - 2) p.Vy_out[Nx + (int64_t)(j + 1) * LD] = vn;
+        }
+        // constant free-slip entries: bc_x_zero!(Vx) and bc_y_zero!(Vy), corners included
+        if (i == 0 || i == Nx - 2) {
+            int ic = (i == 0) ? 0 : Nx - 1;
+            p.Vx_out[ic + (int64_t)(j + 1) * LD] = 0.0;
+            if (j == 0) p.Vx_out[ic] = 0.0;
+            if (j == Ny - 2) p.Vx_out[ic + (int64_t)Ny * LD] = 0.0;
+        }
+        if (j == 0 || j == Ny - 2) {
+            int64_t jr = (j == 0) ? 0 : (int64_t)(Ny - 1) * LD;
+            p.Vy_out[(i + 1) + jr] = 0.0;
+            if (i == 0) p.Vy_out[jr] = 0.0;
+            if (i == Nx - 2) p.Vy_out[Nx + jr] = 0.0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// residuals + norms (compute_Residuals! :241-249, compute_err :103-109)
+// ---------------------------------------------------------------------------
+constexpr int RES_THREADS = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (warp == 0) {
+        r = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+struct ResParams {
+    const double* __restrict__ txx;
+    const double* __restrict__ tyy;
+    const double* __restrict__ txy;
+    const double* __restrict__ P;
+    const double* __restrict__ rho;
+    const double* __restrict__ Vx;
+    const double* __restrict__ Vy;
+    const double* __restrict__ divV;
+    const double* __restrict__ dt_ptr;
+    double* __restrict__ Rx;
+    double* __restrict__ Ry;
+    double* __restrict__ partials;  // [gridDim.x][3]
+    int Nx, Ny;
+    int64_t LD;
+    double _dx, _dy, g_y;
+};
+
+__global__ void __launch_bounds__(RES_THREADS) k_residuals(ResParams p) {
+    __shared__ double sh[32];
+    const int Nx = p.Nx, Ny = p.Ny;
+    const int64_t LD = p.LD, W = Nx - 1, npts = (int64_t)(Nx - 1) * (Ny - 1);
+    const double dt = *p.dt_ptr, _dx = p._dx, _dy = p._dy;
+    double srx = 0.0, sry = 0.0, sdv = 0.0;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < npts; n += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(n % W), j = (int)(n / W);
+        int64_t o = i + (int64_t)j * LD;
+        sdv += fabs(p.divV[o]);
+        if (i < Nx - 2) {
+            double Rx = (p.txx[o + 1] - p.txx[o]) * _dx + (p.txy[o + 1 + LD] - p.txy[o + 1]) * _dy
+                        - (p.P[o + 1] - p.P[o]) * _dx;
+            p.Rx[o] = Rx;
+            srx += fabs(Rx);
+        }
+        if (j < Ny - 2) {
+            double av = 0.25 * (p.Vx[o + LD] + p.Vx[o + 1 + LD] + p.Vx[o + 2 * LD] + p.Vx[o + 1 + 2 * LD]);
+            double dxr = p.rho[o + 2 + LD] - p.rho[o + LD];
+            double dyr = p.rho[o + 1 + 2 * LD] - p.rho[o + 1];
+            double Ry = (p.tyy[o + LD] - p.tyy[o]) * _dy + (p.txy[o + 1 + LD] - p.txy[o + LD]) * _dx
+                        - (p.P[o + LD] - p.P[o]) * _dy
+                        + p.g_y * (p.rho[o + 1 + LD] - dt * (av * dxr * 0.5 * _dx + p.Vy[o + 1 + LD] * dyr * 0.5 * _dy));
+            p.Ry[o] = Ry;
+            sry += fabs(Ry);
+        }
+    }
+    double a = block_sum(srx, sh), b = block_sum(sry, sh), c = block_sum(sdv, sh);
+    if (threadIdx.x == 0) {
+        p.partials[blockIdx.x * 3 + 0] = a;
+        p.partials[blockIdx.x * 3 + 1] = b;
+        p.partials[blockIdx.x * 3 + 2] = c;
+    }
+}
+
+// single block: sum partials in a fixed order; err = max of the three means
+__global__ void k_err_finalize(const double* __restrict__ partials, int nblocks, int64_t nrx, int64_t nry,
+                               int64_t ndv, double* __restrict__ scalars) {
+    __shared__ double sh[32];
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[k] += partials[b * 3 + k];
+    double t0 = block_sum(s[0], sh), t1 = block_sum(s[1], sh), t2 = block_sum(s[2], sh);
+    if (threadIdx.x == 0) {
+        double a = t0 / (double)nrx, b = t1 / (double)nry, c = t2 / (double)ndv;
+        double m = a;
+        if (b > m || b != b) m = b;
+        if (c > m || c != c) m = c;
+        if (a != a) m = a;
+        scalars[SC_SUM_RX] = t0;
+        scalars[SC_SUM_RY] = t1;
+        scalars[SC_SUM_DIV] = t2;
+        scalars[SC_ERR] = m;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// max|V| and compute_dt (:118-121)
+// ---------------------------------------------------------------------------
+__global__ void k_maxabs_v(const double* __restrict__ Vx, const double* __restrict__ Vy, int Nx, int Ny, int64_t LD,
+                           unsigned long long* __restrict__ out /* [2] as bits */) {
+    __shared__ unsigned long long sh[2][32];
+    unsigned long long mx = 0, my = 0;
+    const int64_t nvx = (int64_t)Nx * (Ny + 1), nvy = (int64_t)(Nx + 1) * Ny;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nvx; n += stride) {
+        int64_t i = n % Nx, j = n / Nx;
+        unsigned long long b = (unsigned long long)__double_as_longlong(fabs(Vx[i + j * LD]));
+        mx = b > mx ? b : mx;
+    }
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nvy; n += stride) {
+        int64_t i = n % (Nx + 1), j = n / (Nx + 1);
+        unsigned long long b = (unsigned long long)__double_as_longlong(fabs(Vy[i + j * LD]));
+        my = b > my ? b : my;
+    }
+    // non-negative doubles (and +NaN, which sorts above +Inf) order like their bit patterns
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long a = __shfl_down_sync(0xffffffffu, mx, o), c = __shfl_down_sync(0xffffffffu, my, o);
+        mx = a > mx ? a : mx;
+        my = c > my ? c : my;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) { sh[0][warp] = mx; sh[1][warp] = my; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mx = sh[0][w] > mx ? sh[0][w] : mx;
+            my = sh[1][w] > my ? sh[1][w] : my;
+        }
+        atomicMax(&out[0], mx);
+        atomicMax(&out[1], my);
+    }
+}
+
+// dt = maxdisp * min(dx / max|Vx|, dy / max|Vy|); written to every slot in mask
+__global__ void k_dt_finalize(const unsigned long long* __restrict__ maxbits, double maxdisp, double dx, double dy,
+                              double* __restrict__ scalars, int slot_a, int slot_b) {
+    double mvx = __longlong_as_double((long long)maxbits[0]);
+    double mvy = __longlong_as_double((long long)maxbits[1]);
+    double a = dx / mvx, b = dy / mvy;
+    double m = (b < a) ? b : a;
+    if (a != a) m = a;
+    if (b != b) m = b;
+    double dt = maxdisp * m;
+    scalars[SC_MAX_VX] = mvx;
+    scalars[SC_MAX_VY] = mvy;
+    if (slot_a >= 0) scalars[slot_a] = dt;
+    if (slot_b >= 0) scalars[slot_b] = dt;
+}
+
+__global__ void k_set_scalar(double* __restrict__ p, double v) { *p = v; }
+
+// ---------------------------------------------------------------------------
+// pack / unpack between the caller's Julia-layout arrays and the padded layout
+// ---------------------------------------------------------------------------
+__global__ void k_copy2d(double* __restrict__ dst, int64_t ld_dst, const double* __restrict__ src, int64_t ld_src,
+                         int64_t nx, int64_t ny) {
+    int64_t n = nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = k % nx, j = k / nx;
+        dst[i + j * ld_dst] = src[i + j * ld_src];
+    }
+}
+
+// Vx_pad[2:end-1, :] = Vx_s; Vx_pad[1,:] = -Vx_pad[3,:]; Vx_pad[end,:] = -Vx_pad[end-2,:] (:89-92, :278-282)
+__global__ void k_pad_vx(double* __restrict__ pad, const double* __restrict__ Vx, int64_t LD, int Nx, int Ny) {
+    int64_t W = Nx + 2, n = W * (Ny + 1);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = k % W, j = k / W;
+        double v;
+        if (i == 0) v = -Vx[1 + j * LD];
+        else if (i == W - 1) v = -Vx[(Nx - 2) + j * LD];
+        else v = Vx[(i - 1) + j * LD];
+        pad[k] = v;
+    }
+}
+
+// Vy_pad[:, 2:end-1] = Vy_s; Vy_pad[:,1] = -Vy_pad[:,3]; Vy_pad[:,end] = -Vy_pad[:,end-2] (:90-92, :309-313)
+__global__ void k_pad_vy(double* __restrict__ pad, const double* __restrict__ Vy, int64_t LD, int Nx, int Ny) {
+    int64_t W = Nx + 1, n = W * (Ny + 2);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = k % W, j = k / W;
+        double v;
+        if (j == 0) v = -Vy[i + 1 * LD];
+        else if (j == Ny + 1) v = -Vy[i + (int64_t)(Ny - 2) * LD];
+        else v = Vy[i + (j - 1) * LD];
+        pad[k] = v;
+    }
+}
+
+// compute_timesteps! (:128-133) into the caller's dtVx (Nx-2,Ny-1), dtVy (Nx-1,Ny-2), dtPt (Nx-1,Ny-1)
+__global__ void k_timesteps(const double* __restrict__ mup, int64_t LD, int Nx, int Ny, double c_vsc, double c_ptsc,
+                            double max_nxy, double* __restrict__ dtVx, double* __restrict__ dtVy,
+                            double* __restrict__ dtPt) {
+    int64_t W = Nx - 1, n = W * (Ny - 1);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int i = (int)(k % W), j = (int)(k / W);
+        int64_t o = i + (int64_t)j * LD;
+        if (dtVx && i < Nx - 2) dtVx[i + (int64_t)j * (Nx - 2)] = c_vsc / ((mup[o] + mup[o + 1]) * 0.5) / 4.1;
+        if (dtVy && j < Ny - 2) dtVy[i + (int64_t)j * (Nx - 1)] = c_vsc / ((mup[o] + mup[o + LD]) * 0.5) / 4.1;
+        if (dtPt) dtPt[k] = c_ptsc * mup[o] / max_nxy;
+    }
+}
+
+// mean |g_y * rho_vy| over the Ry interior rho_vy[2:Nx, 2:Ny-1] (1-based)
+__global__ void k_rho_scale(const double* __restrict__ rho, int Nx, int Ny, double g_y, double* __restrict__ partials) {
+    __shared__ double sh[32];
+    int64_t W = Nx - 1, n = W * (Ny - 2);
+    double s = 0.0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = k % W + 1, j = k / W + 1;
+        s += fabs(g_y * rho[i + j * (Nx + 1)]);
+    }
+    double t = block_sum(s, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+}
+
+__global__ void k_sum_partials(const double* __restrict__ partials, int n, double div, double* __restrict__ out) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) s += partials[b];
+    double t = block_sum(s, sh);
+    if (threadIdx.x == 0) *out = t / div;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+constexpr int BX = 32, BY = 16, TY = 8;
+
+static unsigned copy_blocks(sf_ctx* ctx, int64_t n) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)ctx->num_sms * 16));
+}
+
+struct Solver {
+    sf_ctx* ctx;
+    cudaStream_t s;
+    Layout L;
+    PTParams pt;
+    ResParams rp;
+    int cur = 0;  // 0: current V/P in A buffers, 1: in B buffers
+    int res_blocks = 0;
+    int maxv_blocks = 0;
+    double maxdisp, dx, dy;
+
+    int launch_iter(bool store) {
+        const double* vxi = L.f(cur ? F_VXB : F_VXA);
+        const double* vyi = L.f(cur ? F_VYB : F_VYA);
+        const double* pi = L.f(cur ? F_PB : F_PA);
+        pt.Vx_in = vxi;
+        pt.Vy_in = vyi;
+        pt.P_in = pi;
+        pt.Vx_out = L.f(cur ? F_VXA : F_VXB);
+        pt.Vy_out = L.f(cur ? F_VYA : F_VYB);
+        pt.P_out = L.f(cur ? F_PA : F_PB);
+        dim3 grid((unsigned)ceil_div(L.Nx - 1, BX), (unsigned)ceil_div(L.Ny - 1, BY));
+        dim3 block(BX, TY);
+        if (store)
+            k_pt_iter<BX, BY, TY, true><<<grid, block, 0, s>>>(pt);
+        else
+            k_pt_iter<BX, BY, TY, false><<<grid, block, 0, s>>>(pt);
+        SF_LAUNCHED(ctx);
+        cur ^= 1;
+        return SF_OK;
+    }
+
+    const double* Vx_cur() const { return L.f(cur ? F_VXB : F_VXA); }
+    const double* Vy_cur() const { return L.f(cur ? F_VYB : F_VYA); }
+    const double* P_cur() const { return L.f(cur ? F_PB : F_PA); }
+
+    int compute_dt(int slot_a, int slot_b) {
+        unsigned long long* bits = (unsigned long long*)(ctx->d_scalars + SC_MAXBITS);
+        SF_CUDA(cudaMemsetAsync(bits, 0, 2 * sizeof(unsigned long long), s));
+        k_maxabs_v<<<maxv_blocks, 256, 0, s>>>(Vx_cur(), Vy_cur(), (int)L.Nx, (int)L.Ny, L.LD, bits);
+        SF_LAUNCHED(ctx);
+        k_dt_finalize<<<1, 1, 0, s>>>(bits, maxdisp, dx, dy, ctx->d_scalars, slot_a, slot_b);
+        SF_LAUNCHED(ctx);
+        return SF_OK;
+    }
+
+    int residuals() {
+        rp.P = P_cur();
+        rp.Vx = Vx_cur();
+        rp.Vy = Vy_cur();
+        k_residuals<<<res_blocks, RES_THREADS, 0, s>>>(rp);
+        SF_LAUNCHED(ctx);
+        int64_t Nx = L.Nx, Ny = L.Ny;
+        k_err_finalize<<<1, 1024, 0, s>>>(rp.partials, res_blocks, (Nx - 2) * (Ny - 1), (Nx - 1) * (Ny - 2),
+                                          (Nx - 1) * (Ny - 1), ctx->d_scalars);
+        SF_LAUNCHED(ctx);
+        return SF_OK;
+    }
+};
+
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int64_t Ny, double g_y, void* stream,
+                             double* scale) {
+    SF_REQUIRE(ctx && rho_vy && scale, "sf_stokes_residual_scale: NULL argument");
+    SF_REQUIRE(Nx >= 3 && Ny >= 3, "sf_stokes_residual_scale: grid too small");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    int nb = (int)std::min<int64_t>(ceil_div((Nx - 1) * (Ny - 2), 256), 1024);
+    if ((rc = ensure(ctx, ctx->partials, (size_t)nb * 8))) return rc;
+    k_rho_scale<<<nb, 256, 0, s>>>(rho_vy, (int)Nx, (int)Ny, g_y, (double*)ctx->partials.ptr);
+    SF_LAUNCHED(ctx);
+    k_sum_partials<<<1, 1024, 0, s>>>((double*)ctx->partials.ptr, nb, (double)((Nx - 1) * (Ny - 2)),
+                                      ctx->d_scalars + SC_SCALE);
+    SF_LAUNCHED(ctx);
+    SF_CUDA(cudaMemcpyAsync(ctx->h_scalars + SC_SCALE, ctx->d_scalars + SC_SCALE, 8, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    *scale = ctx->h_scalars[SC_SCALE];
+    return SF_OK;
+}
+
+int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy, const double* mu_b,
+                    const double* mu_p, double* txx, double* tyy, double* txy, double* divV, double* dtPt, double* Rx,
+                    double* Ry, double* dVxdt, double* dVydt, double* dtVx, double* dtVy, double* Vx_s, double* Vy_s,
+                    double g_y, double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
+                    int use_stab, double eps, int print_info, int64_t iter_max, void* stream, sf_solve_info* info) {
+    SF_REQUIRE(ctx, "sf_solve_stokes: ctx is NULL");
+    SF_REQUIRE(Nx >= 4 && Ny >= 4, "sf_solve_stokes: Nx, Ny must be >= 4");
+    SF_REQUIRE(Nx < (1 << 20) && Ny < (1 << 20), "sf_solve_stokes: Nx, Ny too large");
+    SF_REQUIRE(P && Vx_pad && Vy_pad && rho_vy && mu_b && mu_p && dVxdt && dVydt && Vx_s && Vy_s,
+               "sf_solve_stokes: a state / parameter array is NULL");
+    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_solve_stokes: dx, dy must be positive");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+
+    // ---- layout / scratch ----
+    Solver S;
+    S.ctx = ctx;
+    S.s = s;
+    S.L.Nx = Nx;
+    S.L.Ny = Ny;
+    S.L.LD = round_up(Nx + 2, 32);
+    S.L.rows = Ny + 3;
+    S.L.fstride = S.L.LD * S.L.rows;
+    size_t fbytes = (size_t)S.L.fstride * 8 * F_NUM;
+    bool fresh = fbytes > ctx->fields.bytes;
+    if ((rc = ensure(ctx, ctx->fields, fbytes))) return rc;
+    S.L.base = (double*)ctx->fields.ptr;
+    if (fresh) SF_CUDA(cudaMemsetAsync(ctx->fields.ptr, 0, ctx->fields.bytes, s));
+    S.res_blocks = (int)std::min<int64_t>(ceil_div((Nx - 1) * (Ny - 1), RES_THREADS), (int64_t)ctx->num_sms * 8);
+    S.maxv_blocks = (int)std::min<int64_t>(ceil_div(Nx * (Ny + 1), 256), (int64_t)ctx->num_sms * 8);
+    if ((rc = ensure(ctx, ctx->partials, (size_t)S.res_blocks * 3 * 8))) return rc;
+    S.maxdisp = maxdisp;
+    S.dx = dx;
+    S.dy = dy;
+
+    // ---- constants (:17-27) ----
+    const double Vdmp = 4.0, Vsc = 0.45, Ptsc = 1.0 / 2.0;
+    const double mdxy = std::min(dx, dy);
+    const double min_dxy2 = mdxy * mdxy;
+    const double max_nxy = (double)std::max(Nx, Ny);
+    const double dampX = 1.0 - Vdmp / (double)Nx;
+    const double dampY = 1.0 - Vdmp / (double)Ny;
+    if (!use_stab) dt = 0.0;  // :29-31
+    const int64_t mnxy = std::min(Nx, Ny);
+    const int64_t ncheck = std::min<int64_t>(5 * mnxy, 2000);  // :35
+    const int64_t ndtupdate = 10 * mnxy;                       // :36
+
+    // ---- pack ----
+    const int64_t LD = S.L.LD;
+    struct Pk { int f; const double* src; int64_t nx, ny; } packs[] = {
+        {F_VXA, Vx_s, Nx, Ny + 1}, {F_VYA, Vy_s, Nx + 1, Ny}, {F_PA, P, Nx - 1, Ny - 1},
+        {F_DVX, dVxdt, Nx - 2, Ny - 1}, {F_DVY, dVydt, Nx - 1, Ny - 2}, {F_RHO, rho_vy, Nx + 1, Ny},
+        {F_MUB, mu_b, Nx, Ny}, {F_MUP, mu_p, Nx - 1, Ny - 1}};
+    for (const Pk& k : packs) {
+        k_copy2d<<<copy_blocks(ctx, k.nx * k.ny), 256, 0, s>>>(S.L.f(k.f), LD, k.src, k.nx, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    k_set_scalar<<<1, 1, 0, s>>>(ctx->d_scalars + SC_DT, dt);
+    SF_LAUNCHED(ctx);
+    if (dtVx || dtVy || dtPt) {
+        k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
+                                                                         Vsc * min_dxy2, Ptsc * 4.1, max_nxy, dtVx,
+                                                                         dtVy, dtPt);
+        SF_LAUNCHED(ctx);
+    }
+
+    PTParams& pt = S.pt;
+    pt.dVx = S.L.f(F_DVX);
+    pt.dVy = S.L.f(F_DVY);
+    pt.rho = S.L.f(F_RHO);
+    pt.mub = S.L.f(F_MUB);
+    pt.mup = S.L.f(F_MUP);
+    pt.txx = S.L.f(F_TXX);
+    pt.tyy = S.L.f(F_TYY);
+    pt.txy = S.L.f(F_TXY);
+    pt.divV = S.L.f(F_DIV);
+    pt.dt_ptr = ctx->d_scalars + SC_DT;
+    pt.Nx = (int)Nx;
+    pt.Ny = (int)Ny;
+    pt.LD = LD;
+    pt._dx = 1.0 / dx;
+    pt._dy = 1.0 / dy;
+    pt.g_y = g_y;
+    pt.dampX = dampX;
+    pt.dampY = dampY;
+    pt.c_vsc = Vsc * min_dxy2;
+    pt.c_ptsc = Ptsc * 4.1;
+    pt.max_nxy = max_nxy;
+    ResParams& rp = S.rp;
+    rp.txx = S.L.f(F_TXX);
+    rp.tyy = S.L.f(F_TYY);
+    rp.txy = S.L.f(F_TXY);
+    rp.rho = S.L.f(F_RHO);
+    rp.divV = S.L.f(F_DIV);
+    rp.dt_ptr = ctx->d_scalars + SC_DT_CHECK;
+    rp.Rx = S.L.f(F_RX);
+    rp.Ry = S.L.f(F_RY);
+    rp.partials = (double*)ctx->partials.ptr;
+    rp.Nx = (int)Nx;
+    rp.Ny = (int)Ny;
+    rp.LD = LD;
+    rp._dx = pt._dx;
+    rp._dy = pt._dy;
+    rp.g_y = g_y;
+
+    // ---- PT loop (:43-77) ----
+    double err = 2.0 * eps;
+    int64_t iter = 1, niter = 0, nchecks = 0;
+    const int64_t itert1 = 11;
+    bool have_t1 = false;
+    int64_t fused = 0;
+    SF_CUDA(cudaEventRecord(ctx->ev_c, s));
+    while (err > eps && iter <= iter_max) {
+        // iterations up to and including the next check (or iter_max)
+        int64_t next_check = ((iter - 1) / ncheck + 1) * ncheck;
+        int64_t last = std::min(next_check, iter_max);
+        for (int64_t it = iter; it <= last; ++it) {
+            if (it == itert1) {
+                SF_CUDA(cudaEventRecord(ctx->ev_a, s));
+                have_t1 = true;
+            }
+            bool store = (it % ncheck == 0) || (it == iter_max);
+            if ((rc = S.launch_iter(store))) return rc;
+            ++fused;
+            bool dt_up = use_stab && (it % ndtupdate == 0);
+            bool check = (it % ncheck == 0);
+            if (dt_up || (check && use_stab)) {
+                if ((rc = S.compute_dt(dt_up ? SC_DT : -1, check ? SC_DT_CHECK : -1))) return rc;
+            }
+            if (check && !use_stab) {
+                k_set_scalar<<<1, 1, 0, s>>>(ctx->d_scalars + SC_DT_CHECK, 0.0);
+                SF_LAUNCHED(ctx);
+            }
+        }
+        niter += last - iter + 1;
+        iter = last + 1;
+        if (last % ncheck == 0) {
+            if ((rc = S.residuals())) return rc;
+            ++nchecks;
+            SF_CUDA(cudaMemcpyAsync(ctx->h_scalars + SC_ERR, ctx->d_scalars + SC_ERR, 8, cudaMemcpyDeviceToHost, s));
+            SF_CUDA(cudaStreamSynchronize(s));
+            err = ctx->h_scalars[SC_ERR];
+            if (!(err == err) || std::isinf(err)) break;
+        }
+    }
+    SF_CUDA(cudaEventRecord(ctx->ev_b, s));
+
+    // ---- unpack (:89-95) ----
+    struct Uk { double* dst; const double* src; int64_t nx, ny; } unpacks[] = {
+        {Vx_s, S.Vx_cur(), Nx, Ny + 1}, {Vy_s, S.Vy_cur(), Nx + 1, Ny}, {P, S.P_cur(), Nx - 1, Ny - 1},
+        {dVxdt, S.L.f(F_DVX), Nx - 2, Ny - 1}, {dVydt, S.L.f(F_DVY), Nx - 1, Ny - 2},
+        {txx, S.L.f(F_TXX), Nx - 1, Ny - 1}, {tyy, S.L.f(F_TYY), Nx - 1, Ny - 1}, {txy, S.L.f(F_TXY), Nx, Ny},
+        {divV, S.L.f(F_DIV), Nx - 1, Ny - 1},
+        {nchecks ? Rx : nullptr, S.L.f(F_RX), Nx - 2, Ny - 1}, {nchecks ? Ry : nullptr, S.L.f(F_RY), Nx - 1, Ny - 2}};
+    for (const Uk& k : unpacks) {
+        if (!k.dst || niter == 0 && (k.src == S.L.f(F_TXX) || k.src == S.L.f(F_TYY) || k.src == S.L.f(F_TXY) ||
+                                     k.src == S.L.f(F_DIV)))
+            continue;
+        k_copy2d<<<copy_blocks(ctx, k.nx * k.ny), 256, 0, s>>>(k.dst, k.nx, k.src, LD, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    k_pad_vx<<<copy_blocks(ctx, (Nx + 2) * (Ny + 1)), 256, 0, s>>>(Vx_pad, S.Vx_cur(), LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    k_pad_vy<<<copy_blocks(ctx, (Nx + 1) * (Ny + 2)), 256, 0, s>>>(Vy_pad, S.Vy_cur(), LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    if ((rc = S.compute_dt(SC_DT_OUT, -1))) return rc;  // returned dt (:95)
+    SF_CUDA(cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, SC_N * 8, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    double dt_out = ctx->h_scalars[SC_DT_OUT];
+
+    float ms_loop = 0.f, ms_t1 = 0.f;
+    SF_CUDA(cudaEventElapsedTime(&ms_loop, ctx->ev_c, ctx->ev_b));
+    if (have_t1) SF_CUDA(cudaEventElapsedTime(&ms_t1, ctx->ev_a, ctx->ev_b));
+    double runtime = have_t1 ? ms_t1 * 1e-3 : 0.0;
+    double t_it = (niter - itert1 + 1) > 0 ? runtime / (double)(niter - itert1 + 1) : 0.0;
+    double A_eff = (3.0 * 2.0) / 1e9 * (double)Nx * (double)Ny * 8.0;
+    double T_eff = t_it > 0 ? A_eff / t_it : 0.0;
+    // essential bytes: read+write Vx_s, Vy_s, P, dVx, dVy; read rho, mu_b, mu_p
+    double bpi = 8.0 * (2.0 * ((double)Nx * (Ny + 1) + (double)(Nx + 1) * Ny + (double)(Nx - 1) * (Ny - 1) +
+                               (double)(Nx - 2) * (Ny - 1) + (double)(Nx - 1) * (Ny - 2)) +
+                        (double)(Nx + 1) * Ny + (double)Nx * Ny + (double)(Nx - 1) * (Ny - 1));
+    if (print_info)
+        printf("Total steps = %lld, err = %1.3e, time = %1.3e sec (@ T_eff = %1.2f GB/s) \n", (long long)niter, err,
+               runtime, T_eff);
+    if (info) {
+        info->dt = dt_out;
+        info->T_eff = T_eff;
+        info->runtime = runtime;
+        info->iters = niter;
+        info->err = err;
+        info->n_checks = nchecks;
+        info->converged = (err <= eps) ? 1 : 0;
+        info->reserved = 0;
+        info->loop_ms = ms_loop;
+        info->bytes_per_iter = bpi;
+        info->T_eff_essential = ms_loop > 0 ? bpi * (double)niter / (ms_loop * 1e-3) / 1e9 : 0.0;
+        info->fused_launches = fused;
+        info->fused_ms = 0.0;
+    }
+    if (!(err == err) || std::isinf(err)) return fail(SF_ERR_NONFINITE, "sf_solve_stokes: residual is not finite");
+    return SF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+"""ctypes binding of libstokesflow_b200.so (the C ABI in include/stokesflow_b200.h).
+
+The library is built in-tree by ``stokesflow.jl_b200/csrc/Makefile`` into
+``stokesflow.jl_b200/lib/``.  There is no fallback: if the shared library is
+missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+_PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG_ROOT, "lib", "libstokesflow_b200.so")
+CSRC = os.path.join(_PKG_ROOT, "csrc")
+
+SF_OK = 0
+SF_ERR_INVALID_ARG = 1
+SF_ERR_CUDA = 2
+SF_ERR_OOM = 3
+SF_ERR_NO_DEVICE = 4
+SF_ERR_NONFINITE = 5
+SF_ERR_TOO_LARGE = 6
+
+_d = C.c_double
+_i64 = C.c_int64
+_i32 = C.c_int32
+_vp = C.c_void_p
+_pd = C.c_void_p  # device pointers are passed as integers
+
+
+class SolveInfo(C.Structure):
+    """sf_solve_info."""
+    _fields_ = [("dt", _d), ("T_eff", _d), ("runtime", _d), ("iters", _i64), ("err", _d), ("n_checks", _i64),
+                ("converged", _i32), ("reserved", _i32), ("loop_ms", _d), ("bytes_per_iter", _d),
+                ("T_eff_essential", _d), ("fused_launches", _i64), ("fused_ms", _d)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Warnings(C.Structure):
+    """sf_warnings."""
+    _fields_ = [("bad_markers", _i64), ("empty_nodes", _i64), ("interp_failsafe", _i64), ("markers_outside", _i64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class PlumeModelC(C.Structure):
+    """sf_plume_model."""
+    _fields_ = [(n, _d) for n in ("air_height", "plume_x", "plume_y", "plume_r", "rho_air", "rho_matrix",
+                                  "rho_plume", "mu_air", "mu_matrix", "mu_plume")]
+
+
+# name -> (restype, argtypes); mirrors include/stokesflow_b200.h
+PROTOTYPES = {
+    "sf_version": (C.c_int, []),
+    "sf_status_string": (C.c_char_p, [C.c_int]),
+    "sf_last_error": (C.c_char_p, []),
+    "sf_ctx_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "sf_ctx_destroy": (C.c_int, [_vp]),
+    "sf_ctx_scratch_bytes": (C.c_int, [_vp, C.POINTER(_i64)]),
+    "sf_ctx_launch_count": (C.c_int, [_vp, C.POINTER(_i64)]),
+    "sf_get_warnings": (C.c_int, [_vp, C.POINTER(Warnings), C.c_int]),
+    "sf_bilinear_marker_to_grid": (C.c_int, [_vp, _d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _pd, _pd,
+                                             _i64, _i64, _vp]),
+    "sf_solve_stokes": (C.c_int, [_vp] + [_pd] * 19 + [_d, _d, _d, _i64, _i64, _d, _d, C.c_int, _d, C.c_int, _i64,
+                                                       _vp, C.POINTER(SolveInfo)]),
+    "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),
+    "sf_move_markers_rk4": (C.c_int, [_vp, _pd, _pd, _i64, _pd, _i64, _i64, _pd, _i64, _i64, _d, _d, _d, _d, _d, _d,
+                                      _d, _d, _d, _vp]),
+    "sf_rebin_markers": (C.c_int, [_vp, _pd, _pd, _i64, _d, _d, _d, _d, _i64, _i64, _pd, _pd, _pd, _vp]),
+    "sf_marker_count": (C.c_int, [_i64, _i64, _i64, C.POINTER(_i64), C.POINTER(_i64)]),
+    "sf_init_markers_host": (C.c_int, [_i64, _d, _d, _d, _d, _i64, _i64, _d, C.c_uint64, _vp, _vp]),
+    "sf_init_markers": (C.c_int, [_vp, _i64, _d, _d, _d, _d, _i64, _i64, _d, C.c_uint64, _pd, _pd, _vp]),
+    "sf_uniform": (_d, [C.c_uint64, C.c_uint64]),
+    "sf_set_marker_properties_host": (C.c_int, [C.POINTER(PlumeModelC), _vp, _vp, _i64, _d, _d, _vp, _vp]),
+    "sf_set_marker_properties": (C.c_int, [_vp, C.POINTER(PlumeModelC), _pd, _pd, _i64, _d, _d, _pd, _pd, _vp]),
+}
+
+_lib = None
+
+
+class StokesFlowError(RuntimeError):
+    """A non-zero sf_status from the library."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+def build(force: bool = False) -> str:
+    """Compile the shared library with csrc/Makefile (nvcc, sm_100a)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", CSRC, "-j4"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Load libstokesflow_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libstokesflow_b200.so not built: {LIB_PATH} missing "
+                               "(run `make -C stokesflow.jl_b200/csrc` or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, what: str = ""):
+    if status != SF_OK:
+        msg = lib().sf_last_error().decode(errors="replace")
+        raise StokesFlowError(status, f"{what}: {msg}" if what else msg)

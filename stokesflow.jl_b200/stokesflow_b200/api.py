@@ -1,0 +1,306 @@
+"""Python mirror of the reference's hot-path functions on CUDA tensors.
+
+Each function keeps the name (snake_case), argument order, meaning and
+in-place behaviour of its Julia counterpart and calls straight into
+libstokesflow_b200.so:
+
+=========================================  =====================================================
+reference (dastrm/StokesFlow.jl)           here
+=========================================  =====================================================
+bilinearMarkerToGrid!  MarkerToGrid.jl:18  :func:`bilinear_marker_to_grid`
+solveStokes!  StokesSolver_multixpu.jl:14  :func:`solve_stokes` (returns ``(dt, T_eff, runtime)``)
+moveMarkersRK4!  MoveMarkers.jl:15         :func:`move_markers_rk4`
+initializeMarkersCPU  common.jl:40         :func:`initialize_markers`
+setInitialMarkerProperties!  common.jl:104 :func:`set_initial_marker_properties`
+exchangeMarkers  MarkerExchange.jl:8       identity on a single domain (not needed)
+=========================================  =====================================================
+
+Grid arrays are float64 CUDA tensors with the Julia shape ``(nx, ny)`` in
+column-major storage (strides ``(1, nx)``), so ``A[ix-1, iy-1]`` is Julia's
+``A[ix, iy]``; :func:`zeros` makes them.  Marker arrays are 1-D contiguous
+float64 CUDA tensors.  Work is queued on the current torch CUDA stream; the
+solve synchronises it (its stopping test reads the residual on the host).
+The MPI ``comm`` / ImplicitGlobalGrid ``grid`` arguments are accepted and
+ignored: the domain is a single rank.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+__all__ = ["Context", "default_context", "zeros", "bilinear_marker_to_grid", "solve_stokes", "solve_stokes_info",
+           "residual_scale", "move_markers_rk4", "rebin_markers", "marker_count", "initialize_markers",
+           "initialize_markers_host", "set_initial_marker_properties", "get_warnings", "PlumeModel"]
+
+
+class Context:
+    """Owns an sf_ctx (device scratch) on one CUDA device."""
+
+    def __init__(self, device: int | None = None):
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = int(device)
+        h = C.c_void_p()
+        check(lib().sf_ctx_create(self.device, C.byref(h)), "sf_ctx_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            lib().sf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def launch_count(self) -> int:
+        """Kernels launched through this context so far."""
+        n = C.c_int64()
+        check(lib().sf_ctx_launch_count(self.handle, C.byref(n)))
+        return n.value
+
+    def scratch_bytes(self) -> int:
+        b = C.c_int64()
+        check(lib().sf_ctx_scratch_bytes(self.handle, C.byref(b)))
+        return b.value
+
+
+_ctx_lock = threading.Lock()
+_contexts: dict[int, Context] = {}
+
+
+def default_context(device: int | None = None) -> Context:
+    if device is None:
+        device = torch.cuda.current_device()
+    with _ctx_lock:
+        ctx = _contexts.get(int(device))
+        if ctx is None:
+            ctx = _contexts[int(device)] = Context(device)
+        return ctx
+
+
+def zeros(*shape, device="cuda") -> torch.Tensor:
+    """Julia ``@zeros(nx, ny)``: float64, column-major, Julia shape."""
+    if len(shape) == 1 and isinstance(shape[0], (tuple, list)):
+        shape = tuple(shape[0])
+    if len(shape) == 1:
+        return torch.zeros(shape[0], dtype=torch.float64, device=device)
+    nx, ny = shape
+    return torch.zeros((ny, nx), dtype=torch.float64, device=device).t()
+
+
+def _grid(a: torch.Tensor, name: str, shape=None) -> int:
+    if a.dtype != torch.float64 or not a.is_cuda:
+        raise TypeError(f"{name}: need a float64 CUDA tensor")
+    if a.dim() != 2 or a.stride() != (1, a.shape[0]):
+        raise ValueError(f"{name}: need a column-major (nx, ny) tensor (strides (1, nx)); got strides {a.stride()}")
+    if shape is not None and tuple(a.shape) != tuple(shape):
+        raise ValueError(f"{name}: shape {tuple(a.shape)} != expected {tuple(shape)}")
+    return a.data_ptr()
+
+
+def _opt_grid(a, name, shape):
+    return None if a is None else _grid(a, name, shape)
+
+
+def _vec(a: torch.Tensor, name: str) -> int:
+    if a.dtype != torch.float64 or not a.is_cuda or a.dim() != 1 or not a.is_contiguous():
+        raise TypeError(f"{name}: need a contiguous 1-D float64 CUDA tensor")
+    return a.data_ptr()
+
+
+def _stream(stream=None) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+def _ctx(ctx: Context | None) -> Context:
+    return ctx if ctx is not None else default_context()
+
+
+# ---------------------------------------------------------------------------
+def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, dx, dy, val_wt_sum=None,
+                            wt_sum=None, grid=None, *, ctx: Context | None = None, stream=None):
+    """bilinearMarkerToGrid! (MarkerToGrid.jl:18-38): deposit val_m onto val_grid in place."""
+    nx, ny = val_grid.shape
+    pg = _grid(val_grid, "val_grid")
+    nm = x_m.numel()
+    px, py, pv = _vec(x_m, "x_m"), _vec(y_m, "y_m"), _vec(val_m, "val_m")
+    if y_m.numel() != nm or val_m.numel() != nm:
+        raise ValueError("x_m, y_m, val_m must have the same length")  # MarkerToGrid.jl:22
+    if (val_wt_sum is None) != (wt_sum is None):
+        raise ValueError("give both val_wt_sum and wt_sum or neither")
+    ps = pw = None
+    ld = n_sum = 0
+    if wt_sum is not None:
+        ps = _grid(val_wt_sum, "val_wt_sum")
+        pw = _grid(wt_sum, "wt_sum", val_wt_sum.shape)
+        ld, n_sum = wt_sum.shape[0], wt_sum.numel()
+    c = _ctx(ctx)
+    check(lib().sf_bilinear_marker_to_grid(c.handle, float(x_grid_min), float(y_grid_min), pg, nx, ny, px, py, pv,
+                                           nm, float(dx), float(dy), ps, pw, ld, n_sum, _stream(stream)),
+          "bilinear_marker_to_grid")
+
+
+def solve_stokes_info(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt, dtVx,
+                      dtVy, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp, comm=None, *,
+                      use_free_surface_stabilization=True, eps=1e-8, print_info=False, iter_max=100000,
+                      ctx: Context | None = None, stream=None) -> dict:
+    """solveStokes! (StokesSolver_multixpu.jl:14-96); returns the full sf_solve_info as a dict.
+    The work arrays txx ... dtVy may be None."""
+    Nx, Ny = int(Nx), int(Ny)
+    ptrs = [
+        _grid(P, "P", (Nx - 1, Ny - 1)), _grid(Vx_pad, "Vx_pad", (Nx + 2, Ny + 1)),
+        _grid(Vy_pad, "Vy_pad", (Nx + 1, Ny + 2)), _grid(rho_vy, "rho_vy", (Nx + 1, Ny)),
+        _grid(mu_b, "mu_b", (Nx, Ny)), _grid(mu_p, "mu_p", (Nx - 1, Ny - 1)),
+        _opt_grid(txx, "txx", (Nx - 1, Ny - 1)), _opt_grid(tyy, "tyy", (Nx - 1, Ny - 1)),
+        _opt_grid(txy, "txy", (Nx, Ny)), _opt_grid(divV, "divV", (Nx - 1, Ny - 1)),
+        _opt_grid(dtPt, "dtPt", (Nx - 1, Ny - 1)), _opt_grid(Rx, "Rx", (Nx - 2, Ny - 1)),
+        _opt_grid(Ry, "Ry", (Nx - 1, Ny - 2)), _grid(dVxdt, "dVxdt", (Nx - 2, Ny - 1)),
+        _grid(dVydt, "dVydt", (Nx - 1, Ny - 2)), _opt_grid(dtVx, "dtVx", (Nx - 2, Ny - 1)),
+        _opt_grid(dtVy, "dtVy", (Nx - 1, Ny - 2)), _grid(Vx_s, "Vx_s", (Nx, Ny + 1)),
+        _grid(Vy_s, "Vy_s", (Nx + 1, Ny)),
+    ]
+    info = _lib.SolveInfo()
+    c = _ctx(ctx)
+    check(lib().sf_solve_stokes(c.handle, *ptrs, float(g_y), float(dx), float(dy), Nx, Ny, float(dt), float(maxdisp),
+                                int(bool(use_free_surface_stabilization)), float(eps), int(bool(print_info)),
+                                int(iter_max), _stream(stream), C.byref(info)), "solve_stokes")
+    return info.as_dict()
+
+
+def solve_stokes(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt, dtVx, dtVy,
+                 Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp, comm=None, *, use_free_surface_stabilization=True,
+                 eps=1e-8, print_info=True, iter_max=100000, ctx: Context | None = None, stream=None):
+    """solveStokes! (StokesSolver_multixpu.jl:14-96) -> (dt, T_eff, runtime)."""
+    r = solve_stokes_info(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt,
+                          dtVx, dtVy, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp, comm,
+                          use_free_surface_stabilization=use_free_surface_stabilization, eps=eps,
+                          print_info=print_info, iter_max=iter_max, ctx=ctx, stream=stream)
+    return r["dt"], r["T_eff"], r["runtime"]
+
+
+def residual_scale(rho_vy, Nx, Ny, g_y, *, ctx: Context | None = None, stream=None) -> float:
+    """mean |g_y rho_vy| over the Ry interior: eps = rtol * residual_scale(...) is a relative stopping test."""
+    out = C.c_double()
+    c = _ctx(ctx)
+    check(lib().sf_stokes_residual_scale(c.handle, _grid(rho_vy, "rho_vy", (Nx + 1, Ny)), int(Nx), int(Ny),
+                                         float(g_y), _stream(stream), C.byref(out)), "residual_scale")
+    return out.value
+
+
+def move_markers_rk4(x_m, y_m, Vx, Vy, x_vx_min, y_vx_min, x_vy_min, y_vy_min, dt, lx, ly, dx, dy, *,
+                     ctx: Context | None = None, stream=None):
+    """moveMarkersRK4! (MoveMarkers.jl:15-23): advect x_m, y_m in place."""
+    nm = x_m.numel()
+    if y_m.numel() != nm:
+        raise ValueError("x and y Marker coords have not same length")  # MoveMarkers.jl:18
+    c = _ctx(ctx)
+    check(lib().sf_move_markers_rk4(c.handle, _vec(x_m, "x_m"), _vec(y_m, "y_m"), nm, _grid(Vx, "Vx"), Vx.shape[0],
+                                    Vx.shape[1], _grid(Vy, "Vy"), Vy.shape[0], Vy.shape[1], float(x_vx_min),
+                                    float(y_vx_min), float(x_vy_min), float(y_vy_min), float(dt), float(lx),
+                                    float(ly), float(dx), float(dy), _stream(stream)), "move_markers_rk4")
+
+
+def rebin_markers(x_m, y_m, x_grid_min, y_grid_min, dx, dy, nx, ny, *, ctx: Context | None = None, stream=None):
+    """Stable counting sort of the markers by cell of an (nx, ny)-node grid.
+    Returns int32 CUDA tensors (counts[(nx+1)*(ny+1)], offsets[+1], perm[nm])."""
+    nm = x_m.numel()
+    ncells = (nx + 1) * (ny + 1)
+    dev = x_m.device
+    counts = torch.empty(ncells, dtype=torch.int32, device=dev)
+    offsets = torch.empty(ncells + 1, dtype=torch.int32, device=dev)
+    perm = torch.empty(max(nm, 1), dtype=torch.int32, device=dev)
+    c = _ctx(ctx)
+    check(lib().sf_rebin_markers(c.handle, _vec(x_m, "x_m"), _vec(y_m, "y_m"), nm, float(x_grid_min),
+                                 float(y_grid_min), float(dx), float(dy), int(nx), int(ny), counts.data_ptr(),
+                                 offsets.data_ptr(), perm.data_ptr(), _stream(stream)), "rebin_markers")
+    return counts, offsets, perm[:nm]
+
+
+def get_warnings(reset: bool = False, *, ctx: Context | None = None) -> dict:
+    w = _lib.Warnings()
+    c = _ctx(ctx)
+    check(lib().sf_get_warnings(c.handle, C.byref(w), int(bool(reset))), "get_warnings")
+    return w.as_dict()
+
+
+# ---------------------------------------------------------------------------
+# markers (common.jl:40-110)
+# ---------------------------------------------------------------------------
+def marker_count(marker_density, nx, ny):
+    a, b = C.c_int64(), C.c_int64()
+    check(lib().sf_marker_count(int(marker_density), int(nx), int(ny), C.byref(a), C.byref(b)), "marker_count")
+    return a.value, b.value
+
+
+def initialize_markers(marker_density, lx, ly, dx, dy, nx, ny, jitter=0.0, seed=0, *, device="cuda",
+                       ctx: Context | None = None, stream=None):
+    """initializeMarkersCPU (common.jl:40-90, one rank), generated on the device.
+    jitter: width of the uniform jitter in marker sub-spacings (reference: 1.0, RAND_MARKER_POS=false: 0.0)."""
+    nmx, nmy = marker_count(marker_density, nx, ny)
+    x = torch.empty(nmx * nmy, dtype=torch.float64, device=device)
+    y = torch.empty_like(x)
+    c = _ctx(ctx)
+    check(lib().sf_init_markers(c.handle, int(marker_density), float(lx), float(ly), float(dx), float(dy), int(nx),
+                                int(ny), float(jitter), int(seed), x.data_ptr(), y.data_ptr(), _stream(stream)),
+          "initialize_markers")
+    return x, y
+
+
+def initialize_markers_host(marker_density, lx, ly, dx, dy, nx, ny, jitter=0.0, seed=0):
+    """Same as :func:`initialize_markers` into pinned host tensors (for the end-to-end path)."""
+    nmx, nmy = marker_count(marker_density, nx, ny)
+    x = torch.empty(nmx * nmy, dtype=torch.float64, pin_memory=torch.cuda.is_available())
+    y = torch.empty_like(x)
+    check(lib().sf_init_markers_host(int(marker_density), float(lx), float(ly), float(dx), float(dy), int(nx),
+                                     int(ny), float(jitter), int(seed), C.c_void_p(x.data_ptr()),
+                                     C.c_void_p(y.data_ptr())), "initialize_markers_host")
+    return x, y
+
+
+class PlumeModel:
+    """Layered 'sticky air' + circular plume + matrix material model
+    (StokesFlow2D_multixpu.jl:382-404): y < air_height -> air, else inside the
+    plume circle -> plume, else matrix."""
+
+    FIELDS = ("air_height", "plume_x", "plume_y", "plume_r", "rho_air", "rho_matrix", "rho_plume", "mu_air",
+              "mu_matrix", "mu_plume")
+
+    def __init__(self, **kw):
+        for f in self.FIELDS:
+            setattr(self, f, float(kw[f]))
+
+    def c(self):
+        return _lib.PlumeModelC(*[getattr(self, f) for f in self.FIELDS])
+
+    def __repr__(self):
+        return "PlumeModel(" + ", ".join(f"{f}={getattr(self, f)!r}" for f in self.FIELDS) + ")"
+
+
+def set_initial_marker_properties(x_m, y_m, model: PlumeModel, x0=0.0, y0=0.0, *, ctx: Context | None = None,
+                                  stream=None):
+    """setInitialMarkerProperties! (common.jl:104-110) -> (rho_m, mu_m) on the markers' device."""
+    nm = x_m.numel()
+    rho = torch.empty_like(x_m)
+    mu = torch.empty_like(x_m)
+    cm = model.c()
+    if x_m.is_cuda:
+        c = _ctx(ctx)
+        check(lib().sf_set_marker_properties(c.handle, C.byref(cm), _vec(x_m, "x_m"), _vec(y_m, "y_m"), nm,
+                                             float(x0), float(y0), rho.data_ptr(), mu.data_ptr(), _stream(stream)),
+              "set_initial_marker_properties")
+    else:
+        assert x_m.dtype == torch.float64 and x_m.is_contiguous() and y_m.is_contiguous()
+        check(lib().sf_set_marker_properties_host(C.byref(cm), C.c_void_p(x_m.data_ptr()), C.c_void_p(y_m.data_ptr()),
+                                                  nm, float(x0), float(y0), C.c_void_p(rho.data_ptr()),
+                                                  C.c_void_p(mu.data_ptr())), "set_initial_marker_properties")
+    return rho, mu

@@ -1,0 +1,295 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Deposit, PT iterates and marker positions are expected BIT-IDENTICAL to the
+oracle (same expression order, no FMA contraction, reference summation order
+in the deposit).  The only floating-point difference allowed anywhere is the
+summation order inside the residual norm `err`, which can only move the
+stopping iteration when err lands within ~1e-15 of eps; the full-timestep
+tests therefore also check the north-star bar (1e-10 relative L2) explicitly.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from fields import F, golden, random_fields, rel_l2, solver_test_fields
+
+pytestmark = pytest.mark.gpu
+
+TOL_REL_L2 = 1e-10   # plain FP64 path vs oracle, V / P / marker positions
+
+
+def dev(a: np.ndarray) -> torch.Tensor:
+    """numpy (Julia layout, Fortran order) -> column-major CUDA tensor of the same shape."""
+    a = np.asarray(a, dtype=np.float64)
+    if a.ndim == 1:
+        return torch.from_numpy(a.copy()).cuda()
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+
+def host(t: torch.Tensor) -> np.ndarray:
+    if t.dim() == 1:
+        return t.cpu().numpy()
+    return np.asfortranarray(t.t().contiguous().cpu().numpy().T)
+
+
+# ---------------------------------------------------------------------------
+# deposit
+# ---------------------------------------------------------------------------
+def test_deposit_kat(sf):
+    g = golden()["marker_to_grid_kat"]
+    val = sf.zeros(*g["shape"])
+    vws = dev(np.ones(g["shape"], order="F"))
+    ws = dev(np.ones(g["shape"], order="F"))
+    sf.bilinear_marker_to_grid(g["x_grid_min"], g["y_grid_min"], val, dev(np.array(g["x_m"])),
+                               dev(np.array(g["y_m"])), dev(np.array(g["val_m"])), g["dx"], g["dy"], vws, ws)
+    assert np.allclose(host(val), np.array(g["reference_columns"]).T, rtol=1.5e-8, atol=0)
+
+
+@pytest.mark.parametrize("which", ["rho", "mu_b", "mu_p"])
+def test_deposit_bitexact_random(sf, oracle_lib, which):
+    """Random markers (with 3 erroneous ones) onto each of the three staggered grids."""
+    O = oracle_lib
+    Nx, Ny = 37, 29
+    dx, dy = 1.0 / (Nx - 1), 0.8 / (Ny - 1)
+    o = O.node_origins(dx, dy)
+    x0, y0, shape = {"rho": (o["x_rho"], o["y_rho"], (Nx + 1, Ny)), "mu_b": (o["x"], o["y"], (Nx, Ny)),
+                     "mu_p": (o["x_p"], o["y_p"], (Nx - 1, Ny - 1))}[which]
+    rng = np.random.default_rng(5)
+    nm = 30 * (Nx - 1) * (Ny - 1)
+    x = rng.random(nm) * (Nx - 1) * dx
+    y = rng.random(nm) * (Ny - 1) * dy
+    x[:3] = [-1.0, 5.0, np.nan]
+    v = np.exp(rng.normal(size=nm))
+    ref = np.asfortranarray(rng.random(shape))
+    vws_o, ws_o = F(Nx + 1, Ny), F(Nx + 1, Ny)
+    ref_before = ref.copy(order="F")
+    nb, ne = O.bilinear_marker_to_grid(x0, y0, ref, x, y, v, dx, dy, vws_o, ws_o)
+    got = dev(ref_before)
+    vws, ws = sf.zeros(Nx + 1, Ny), sf.zeros(Nx + 1, Ny)
+    sf.get_warnings(reset=True)
+    sf.bilinear_marker_to_grid(x0, y0, got, dev(x), dev(y), dev(v), dx, dy, vws, ws)
+    w = sf.get_warnings(reset=True)
+    assert np.array_equal(host(got), ref)
+    assert np.array_equal(host(ws), ws_o) and np.array_equal(host(vws), vws_o)
+    assert w["bad_markers"] == nb == 3
+    assert w["empty_nodes"] == ne
+
+
+def test_deposit_no_markers_keeps_values(sf):
+    val = dev(np.full((5, 4), 3.0, order="F"))
+    empty = torch.empty(0, dtype=torch.float64, device="cuda")
+    sf.get_warnings(reset=True)
+    sf.bilinear_marker_to_grid(0.0, 0.0, val, empty, empty, empty, 0.1, 0.1)
+    assert np.all(host(val) == 3.0)
+    assert sf.get_warnings(reset=True)["empty_nodes"] == 20
+
+
+def test_deposit_clustered_markers(sf, oracle_lib):
+    """Many markers in few cells (long segments) and markers exactly on nodes."""
+    O = oracle_lib
+    nx, ny, dx, dy = 8, 6, 0.5, 0.25
+    rng = np.random.default_rng(9)
+    x = np.concatenate([rng.random(3000) * 0.3 + 1.0, np.arange(nx) * dx])
+    y = np.concatenate([rng.random(3000) * 0.2 + 0.5, np.full(nx, 2 * dy)])
+    v = rng.random(x.size)
+    ref = F(nx, ny)
+    O.bilinear_marker_to_grid(0.0, 0.0, ref, x, y, v, dx, dy, F(nx, ny), F(nx, ny))
+    got = sf.zeros(nx, ny)
+    sf.bilinear_marker_to_grid(0.0, 0.0, got, dev(x), dev(y), dev(v), dx, dy)
+    assert np.array_equal(host(got), ref)
+
+
+# ---------------------------------------------------------------------------
+# solver
+# ---------------------------------------------------------------------------
+NAMES = ["P", "Vx", "Vy", "rho_vy", "mu_b", "mu_p", "txx", "tyy", "txy", "divV", "dtPt", "Rx", "Ry", "dVxdt",
+         "dVydt", "dtVx", "dtVy", "Vx_s", "Vy_s"]
+
+
+def gpu_solve(sf, a_np, g_y, dx, dy, Nx, Ny, dt, maxdisp, stab, eps, iter_max):
+    t = {k: dev(v) for k, v in a_np.items()}
+    info = sf.solve_stokes_info(*[t[k] for k in NAMES], g_y, dx, dy, Nx, Ny, dt, maxdisp,
+                                use_free_surface_stabilization=stab, eps=eps, iter_max=iter_max)
+    return {k: host(v) for k, v in t.items()}, info
+
+
+def test_solver_golden(sf, oracle_lib):
+    """test/test_StokesSolver.jl:48-140 on the GPU; bit-identical to the oracle."""
+    O = oracle_lib
+    g = golden()["stokes_solver"]
+    Nx, Ny, dx, dy = g["Nx"], g["Ny"], g["dx"], g["dy"]
+    a = O.stokes_arrays(Nx, Ny)
+    a["rho_vy"][:], a["mu_b"][:], a["mu_p"][:] = solver_test_fields(Nx, Ny, dx, dy)
+    b, info = gpu_solve(sf, {k: v.copy(order="F") for k, v in a.items()}, g["g_y"], dx, dy, Nx, Ny, 0.0,
+                        g["maxdisp"], True, g["eps"], 100000)
+    r = O.solve_stokes(a, g["g_y"], dx, dy, Nx, Ny, 0.0, g["maxdisp"], True, g["eps"], 100000)
+    inds = np.array(g["inds"]) - 1
+    vx = b["Vx"].ravel(order="F")[inds]
+    assert np.linalg.norm(vx - g["vx_ref"]) <= 1.5e-8 * np.linalg.norm(g["vx_ref"])
+    vy = b["Vy"].ravel(order="F")[inds]
+    assert np.linalg.norm(vy - g["vy_ref"]) <= 1.5e-8 * np.linalg.norm(g["vy_ref"])
+    assert info["iters"] == r.iters and info["n_checks"] == r.n_checks and info["converged"] == 1
+    assert info["dt"] == r.dt
+    assert math.isclose(info["err"], r.err, rel_tol=1e-12)
+    for k in NAMES:
+        assert np.array_equal(b[k], a[k]), f"{k} differs from the oracle"
+
+
+@pytest.mark.parametrize("Nx,Ny,iters,stab,dt0", [(67, 45, 700, True, 0.0), (40, 70, 1234, True, 3e-3),
+                                                  (33, 33, 500, False, 0.0), (130, 97, 2100, True, 1e-3)])
+def test_solver_fixed_iterations_bitexact(sf, oracle_lib, Nx, Ny, iters, stab, dt0):
+    """Warm-started solves from a non-trivial state with a 1e3 viscosity contrast, a fixed iteration count
+    (dt updates, checks and a final partial chunk inside), Nx != Ny: every array bit-identical."""
+    O = oracle_lib
+    dx, dy = 1.0 / (Nx - 1), 1.2 / (Ny - 1)
+    a = O.stokes_arrays(Nx, Ny)
+    a["rho_vy"][:], a["mu_b"][:], a["mu_p"][:] = random_fields(Nx, Ny, seed=Nx)
+    rng = np.random.default_rng(Ny)
+    for k in ("P", "Vx_s", "Vy_s", "dVxdt", "dVydt"):
+        a[k][:] = 1e-3 * rng.normal(size=a[k].shape)
+    b, info = gpu_solve(sf, {k: v.copy(order="F") for k, v in a.items()}, 9.81, dx, dy, Nx, Ny, dt0, 0.5, stab,
+                        1e-300, iters)
+    r = O.solve_stokes(a, 9.81, dx, dy, Nx, Ny, dt0, 0.5, stab, 1e-300, iters)
+    assert info["iters"] == r.iters == iters
+    assert info["dt"] == r.dt
+    for k in NAMES:
+        assert np.array_equal(b[k], a[k]), f"{k} differs from the oracle"
+
+
+def test_solver_nonfinite_status(sf):
+    Nx = Ny = 16
+    a = {k: np.zeros(s, order="F") for k, s in _shapes(Nx, Ny).items()}
+    a["rho_vy"][:] = 1.0
+    a["mu_b"][:] = 1.0
+    a["mu_p"][:] = 1.0
+    a["P"][3, 3] = np.nan
+    with pytest.raises(sf.StokesFlowError) as e:
+        gpu_solve(sf, a, 9.81, 0.1, 0.1, Nx, Ny, 0.0, 0.5, True, 1e-8, 10000)
+    assert e.value.status == 5
+
+
+def _shapes(Nx, Ny):
+    return dict(P=(Nx - 1, Ny - 1), Vx=(Nx + 2, Ny + 1), Vy=(Nx + 1, Ny + 2), rho_vy=(Nx + 1, Ny), mu_b=(Nx, Ny),
+                mu_p=(Nx - 1, Ny - 1), txx=(Nx - 1, Ny - 1), tyy=(Nx - 1, Ny - 1), txy=(Nx, Ny),
+                divV=(Nx - 1, Ny - 1), dtPt=(Nx - 1, Ny - 1), Rx=(Nx - 2, Ny - 1), Ry=(Nx - 1, Ny - 2),
+                dVxdt=(Nx - 2, Ny - 1), dVydt=(Nx - 1, Ny - 2), dtVx=(Nx - 2, Ny - 1), dtVy=(Nx - 1, Ny - 2),
+                Vx_s=(Nx, Ny + 1), Vy_s=(Nx + 1, Ny))
+
+
+# ---------------------------------------------------------------------------
+# advection + rebin
+# ---------------------------------------------------------------------------
+def test_advection_bitexact(sf, oracle_lib):
+    O = oracle_lib
+    Nx, Ny = 41, 35
+    dx, dy = 1.0 / (Nx - 1), 1.0 / (Ny - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    rng = np.random.default_rng(2)
+    Vx = np.asfortranarray(rng.normal(size=(Nx + 2, Ny + 1)))
+    Vy = np.asfortranarray(rng.normal(size=(Nx + 1, Ny + 2)))
+    nm = 50000
+    x = rng.random(nm) * lx
+    y = rng.random(nm) * ly
+    x[:4] = [0.0, lx, -0.3, 2.0]   # on / beyond the walls: exercises the clamps and failsafes
+    y[:4] = [ly, 0.0, 0.5, -1.0]
+    dt = 0.5 * min(dx / np.abs(Vx).max(), dy / np.abs(Vy).max())
+    xg, yg = dev(x), dev(y)
+    sf.get_warnings(reset=True)
+    o = O.node_origins(dx, dy)
+    sf.move_markers_rk4(xg, yg, dev(Vx), dev(Vy), o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy)
+    nf = O.move_markers_rk4(x, y, Vx, Vy, o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy)
+    assert np.array_equal(host(xg), x) and np.array_equal(host(yg), y)
+    assert sf.get_warnings(reset=True)["interp_failsafe"] == nf > 0
+
+
+def test_advection_constant_field(sf):
+    """test/test_MoveMarkers.jl:16-47 on the GPU."""
+    Nx, Ny, dx, dy = 10, 13, 0.4, 0.7
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    rng = np.random.default_rng(0)
+    nm = 25 * (Nx - 1) * (Ny - 1)
+    x = rng.random(nm) * (lx - dx) + 0.5 * dx
+    y = rng.random(nm) * (ly - dy) + 0.5 * dy
+    xg, yg = dev(x), dev(y)
+    dt = 0.5 * min(dx / 1.0, dy / 2.0)
+    sf.move_markers_rk4(xg, yg, dev(np.ones((Nx + 2, Ny + 1), order="F")),
+                        dev(-2 * np.ones((Nx + 1, Ny + 2), order="F")), -dx, -0.5 * dy, -0.5 * dx, -dy, dt, lx, ly,
+                        dx, dy)
+    assert np.allclose(host(xg), x + dt, rtol=1.5e-8) and np.allclose(host(yg), y - 2 * dt, rtol=1.5e-8)
+
+
+def test_rebin_counts_and_order(sf, oracle_lib):
+    O = oracle_lib
+    nx, ny, dx, dy = 50, 40, 0.02, 0.025
+    rng = np.random.default_rng(4)
+    nm = 100000
+    x = rng.random(nm) * (nx - 1) * dx
+    y = rng.random(nm) * (ny - 1) * dy
+    x[:2] = [-5.0, 100.0]
+    counts_o, nout = O.cell_counts(x, y, 0.0, 0.0, dx, dy, nx, ny)
+    sf.get_warnings(reset=True)
+    counts, offsets, perm = sf.rebin_markers(dev(x), dev(y), 0.0, 0.0, dx, dy, nx, ny)
+    assert np.array_equal(counts.cpu().numpy(), counts_o)
+    assert sf.get_warnings(reset=True)["markers_outside"] == nout == 2
+    off = offsets.cpu().numpy()
+    p = perm.cpu().numpy()[: off[-1]]
+    assert off[-1] == nm - 2
+    assert np.array_equal(np.sort(p), np.arange(2, nm))
+    for c in range(0, counts_o.size, 97):
+        seg = p[off[c]:off[c + 1]]
+        assert np.all(np.diff(seg) > 0)
+
+
+# ---------------------------------------------------------------------------
+# full timesteps
+# ---------------------------------------------------------------------------
+def test_flow_golden_matches_oracle(sf, oracle_lib):
+    """test/test_StokesFlow2D.jl:53-110 (5 timesteps) on the GPU, against the oracle."""
+    O = oracle_lib
+    g = golden()["stokes_flow_2d"]
+    model = sf.PlumeModel(**g["model"])
+    Vx, Vy, t_tot = sf.stokes_flow_2d(g["Nt"], g["Nx"], g["Ny"], g["Lx"], g["Ly"], model,
+                                      marker_density=g["marker_density"], stokes_eps=g["stokes_eps"])
+    Vxo, Vyo, t_o = O.stokes_flow_2d(g["Nt"], g["Nx"], g["Ny"], g["Lx"], g["Ly"], O.PlumeModel(**g["model"]),
+                                     marker_density=g["marker_density"], stokes_eps=g["stokes_eps"])
+    assert rel_l2(Vx, Vxo) <= TOL_REL_L2 and rel_l2(Vy, Vyo) <= TOL_REL_L2
+    assert math.isclose(t_tot, t_o, rel_tol=1e-12)
+    inds = np.array(g["inds"]) - 1
+    assert np.abs(Vx.ravel(order="F")[inds] - g["vx_ref"]).max() < 6e-4
+
+
+def test_plume_64_five_timesteps(sf, oracle_lib):
+    """The CPU-runnable plume case (63x63 cells, 4x4 markers per cell jittered +-0.25 from seed 0,
+    relative residual 1e-6, 5 timesteps, air viscosity 1e-2) against the oracle:
+    V, P, marker positions within 1e-10 relative L2 and identical markers-per-cell counts."""
+    O = oracle_lib
+    m = sf.plume_model_unit_square()
+    m.mu_air = 1e-2
+    st = sf.StokesFlow2D(64, 64, 1.0, 1.0, m, marker_density=4, stokes_rtol=1e-6, jitter=0.5, seed=0, rebin=True)
+    om = O.PlumeModel(**{f: getattr(m, f) for f in m.FIELDS})
+    dx = dy = 1.0 / 63
+    a = O.stokes_arrays(64, 64)
+    vws, ws = F(65, 64), F(65, 64)
+    o = O.node_origins(dx, dy)
+    x, y = O.initialize_markers(4, 1.0, 1.0, dx, dy, 64, 64, 0.5, 0)
+    rho, mu = O.set_marker_properties(om, x, y)
+    dt = 0.0
+    for _ in range(5):
+        rec = st.step()
+        O.bilinear_marker_to_grid(o["x_rho"], o["y_rho"], a["rho_vy"], x, y, rho, dx, dy, vws, ws)
+        O.bilinear_marker_to_grid(o["x"], o["y"], a["mu_b"], x, y, mu, dx, dy, vws, ws)
+        O.bilinear_marker_to_grid(o["x_p"], o["y_p"], a["mu_p"], x, y, mu, dx, dy, vws, ws)
+        eps = 1e-6 * np.mean(np.abs(9.81 * a["rho_vy"][1:-1, 1:-1]))
+        r = O.solve_stokes(a, 9.81, dx, dy, 64, 64, dt, 0.5, True, eps, 100000)
+        dt = r.dt
+        O.move_markers_rk4(x, y, a["Vx"], a["Vy"], o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, 1.0, 1.0, dx, dy)
+        assert rec["info"]["converged"] == 1 and rec["info"]["iters"] == r.iters
+        for k, t in (("Vx", st.Vx), ("Vy", st.Vy), ("P", st.P)):
+            assert rel_l2(host(t), a[k]) <= TOL_REL_L2, k
+        assert rel_l2(host(st.x_m), x) <= TOL_REL_L2 and rel_l2(host(st.y_m), y) <= TOL_REL_L2
+        counts_o, _ = O.cell_counts(x, y, 0.0, 0.0, dx, dy, 64, 64)
+        assert np.array_equal(st.counts.cpu().numpy(), counts_o)
+    # with every piece bit-identical, so is the whole run
+    assert np.array_equal(host(st.Vx), a["Vx"]) and np.array_equal(host(st.x_m), x)
