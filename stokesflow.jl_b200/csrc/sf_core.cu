@@ -266,6 +266,7 @@ int sf_ctx_create(int device, sf_ctx** out) {
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
     if (cudaMalloc(&c->d_counters, sizeof(unsigned long long) * CNT_N) != cudaSuccess ||
         cudaMalloc(&c->d_scalars, sizeof(double) * SC_N) != cudaSuccess ||
+        cudaMalloc(&c->d_flags, sizeof(int) * 4) != cudaSuccess ||
         cudaMallocHost(&c->h_scalars, sizeof(double) * SC_N) != cudaSuccess ||
         cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess ||
         cudaEventCreate(&c->ev_c) != cudaSuccess || cudaEventCreate(&c->ev_d) != cudaSuccess) {
@@ -275,6 +276,7 @@ int sf_ctx_create(int device, sf_ctx** out) {
     }
     cudaMemset(c->d_counters, 0, sizeof(unsigned long long) * CNT_N);
     cudaMemset(c->d_scalars, 0, sizeof(double) * SC_N);
+    cudaMemset(c->d_flags, 0, sizeof(int) * 4);
     SF_CUDA(cudaDeviceSynchronize());
     *out = c;
     return SF_OK;
@@ -289,6 +291,7 @@ int sf_ctx_destroy(sf_ctx* c) {
         if (s->ptr) cudaFree(s->ptr);
     if (c->d_counters) cudaFree(c->d_counters);
     if (c->d_scalars) cudaFree(c->d_scalars);
+    if (c->d_flags) cudaFree(c->d_flags);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     cudaEvent_t evs[] = {c->ev_a, c->ev_b, c->ev_c, c->ev_d};
     for (cudaEvent_t ev : evs)

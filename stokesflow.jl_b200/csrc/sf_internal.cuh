@@ -71,6 +71,7 @@ struct sf_ctx {
     unsigned long long* d_counters = nullptr;
     double* d_scalars = nullptr;
     double* h_scalars = nullptr;  // pinned mirror
+    int* d_flags = nullptr;       // device error flags (int[4]); [0]: a bounded wait timed out
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
     int64_t launches = 0;         // kernels launched through this context
 };

@@ -5,14 +5,17 @@
 // compute_V! -> four BC kernels (:48-57), with tau, divV, dtau* stored as full
 // arrays.  Here one fused kernel does the whole iteration:
 //
-//   * every CTA owns a BX x BY tile of points (i, j), 0 <= i < Nx-1,
+//   * the domain is cut into BX x BY tiles of points (i, j), 0 <= i < Nx-1,
 //     0 <= j < Ny-1 (the pressure index space, which contains the dVx and dVy
-//     index spaces);
-//   * it stages old Vx, Vy, rho (tile + 2 halo) and old P, mu_p, mu_b
-//     (tile + 1 halo) in shared memory, computes P_new, tau_xx, tau_yy,
-//     tau_xy on the tile + 1 halo (the halo row/column is recomputed by the
-//     neighbouring CTA, which is cheaper than a grid-wide barrier), then the
-//     residuals, the damped rates dV and the new velocities of its tile;
+//     index spaces); persistent CTAs (2 per SM) walk the tiles;
+//   * one thread per CTA brings the next tile's old Vx, Vy, rho, P, mu_p, mu_b
+//     (tile + 2 halo) and dVx, dVy (tile) into a second shared-memory stage
+//     with bulk-tensor copies (TMA, mbarrier-completed) while the CTA computes
+//     the current tile, so the HBM stream never waits for the arithmetic;
+//   * per tile it computes P_new, tau_xx, tau_yy, tau_xy on the tile + 1 halo
+//     (the halo row/column is recomputed by the neighbouring tile, cheaper
+//     than a grid-wide barrier), then the residuals, the damped rates dV and
+//     the new velocities of its tile;
 //   * tau, divV, dtau* are never stored (dtau* is recomputed from mu_p);
 //   * the free-slip ghost rows / columns of the new velocities are written by
 //     the CTAs on the domain edge, in the reference's BC order (:53-56);
@@ -37,6 +40,7 @@
 #include <vector>
 
 #include "sf_internal.cuh"
+#include "sf_tma.cuh"
 
 namespace sf {
 
@@ -74,148 +78,193 @@ struct PTParams {
     double c_vsc;    // Vsc * min_dxy2            (StokesSolver_multixpu.jl:129)
     double c_ptsc;   // Ptsc * 4.1                (:131)
     double max_nxy;  // max(nx_g(), ny_g())       (:21)
+    double inv_max_nxy;  // 1/max_nxy, used only when max_nxy is a power of two (then x/max == x*inv exactly)
+    int pow2;
+    int ntx, nty;        // tiles in x / y
+    int* __restrict__ err_flag;  // set when a tile copy did not arrive in time
 };
 
 // ---------------------------------------------------------------------------
-// fused PT iteration
+// fused PT iteration: persistent CTAs, TMA double-buffered tiles
 // ---------------------------------------------------------------------------
-template <int BX, int BY, int TY, bool STORE>
-__global__ void __launch_bounds__(BX * TY) k_pt_iter(PTParams p) {
-    constexpr int W2 = BX + 2, H2 = BY + 2;  // V / rho tiles
-    constexpr int W1 = BX + 1, H1 = BY + 1;  // P / tau tiles
-    constexpr int NT = BX * TY;
-    __shared__ double sVx[H2][W2];
-    __shared__ double sVy[H2][W2];
-    __shared__ double sRho[H2][W2];
-    __shared__ double sP[H1][W1];     // old P, then new P
-    __shared__ double sMup[H1][W1];
-    __shared__ double sTxy[H1][W1];   // mu_b, then tau_xy
-    __shared__ double sTxx[H1][W1];
-    __shared__ double sTyy[H1][W1];
+// Each CTA walks tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...  While it
+// computes tile t from shared-memory stage s, one thread has already issued
+// the bulk-tensor copies of tile t + gridDim.x into stage s^1, so HBM reads
+// overlap the arithmetic without needing high occupancy.  A stage holds the
+// old Vx, Vy, rho_vy, P, mu_p, mu_b boxes (tile + 2 halo; the TMA zero-fills
+// beyond the arrays) and the dVx, dVy boxes (tile only).
+constexpr int BX = 32, BY = 16, TY = 8;      // owned tile, threads (BX x TY)
+constexpr int TW = BX + 2, TH = BY + 2;      // staged box (tile + 2 halo); TW*8 is a multiple of 16 bytes
+constexpr int W1 = BX + 1, H1 = BY + 1;      // P / tau points computed per tile (tile + 1 halo)
+constexpr int RPT = BY / TY;                 // owned rows per thread
+constexpr int ARR_BYTES = ((TH * TW * 8 + 127) / 128) * 128;
+constexpr int DV_BYTES = ((BY * BX * 8 + 127) / 128) * 128;
+constexpr int ST1_BYTES = ((H1 * W1 * 8 + 127) / 128) * 128;
+constexpr int STAGE_BYTES = 6 * ARR_BYTES + 2 * DV_BYTES;
+constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 2 * BY * BX * 8;  // bytes delivered per stage
+constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 4 * ST1_BYTES + 64;
+constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;                 // 2 s per stage wait
+enum { S_VX = 0, S_VY, S_RHO, S_P, S_MUP, S_MUB };
 
-    const int tid = threadIdx.y * BX + threadIdx.x;
-    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
-    const int Nx = p.Nx, Ny = p.Ny;
+struct TmaMaps {
+    CUtensorMap f[6];  // S_* order
+    CUtensorMap dvx, dvy;
+};
+
+template <bool STORE>
+__global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ TmaMaps maps, PTParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    typedef double Row1[W1];
+    typedef double Row2[TW];
+    typedef double RowD[BX];
+    Row1* sPn = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES);
+    Row1* sTxx = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + ST1_BYTES);
+    Row1* sTyy = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + 2 * ST1_BYTES);
+    Row1* sTxy = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + 3 * ST1_BYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * STAGE_BYTES + 4 * ST1_BYTES);
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+    const int Nx = p.Nx, Ny = p.Ny, ntiles = p.ntx * p.nty;
     const int64_t LD = p.LD;
+    const double _dx = p._dx, _dy = p._dy;
 
-    // ---- owned-point state into registers (issued first) ----
-    constexpr int RPT = BY / TY;  // owned rows per thread
-    double dvx_old[RPT], dvy_old[RPT];
-#pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        int i = i0 + threadIdx.x, j = j0 + threadIdx.y + r * TY;
-        int64_t o = i + (int64_t)j * LD;
-        dvx_old[r] = (i < Nx - 2 && j < Ny - 1) ? p.dVx[o] : 0.0;
-        dvy_old[r] = (i < Nx - 1 && j < Ny - 2) ? p.dVy[o] : 0.0;
-    }
-    // ---- stage tiles ----
-    for (int idx = tid; idx < W2 * H2; idx += NT) {
-        int a = idx % W2, b = idx / W2;
-        int i = i0 + a, j = j0 + b;
-        int64_t o = i + (int64_t)j * LD;
-        sVx[b][a] = (i < Nx && j < Ny + 1) ? p.Vx_in[o] : 0.0;
-        sVy[b][a] = (i < Nx + 1 && j < Ny) ? p.Vy_in[o] : 0.0;
-        sRho[b][a] = (i < Nx + 1 && j < Ny) ? p.rho[o] : 0.0;
-    }
-    for (int idx = tid; idx < W1 * H1; idx += NT) {
-        int a = idx % W1, b = idx / W1;
-        int i = i0 + a, j = j0 + b;
-        int64_t o = i + (int64_t)j * LD;
-        bool pp = (i < Nx - 1 && j < Ny - 1);
-        sP[b][a] = pp ? p.P_in[o] : 0.0;
-        sMup[b][a] = pp ? p.mup[o] : 0.0;
-        sTxy[b][a] = (i < Nx && j < Ny) ? p.mub[o] : 0.0;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
     }
     __syncthreads();
+    auto issue = [&](int t, int s) {  // thread 0 only
+        const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
+        unsigned char* st = smem + s * STAGE_BYTES;
+        mbar_arrive_expect_tx(&bar[s], STAGE_TX);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tma_load_2d(st + k * ARR_BYTES, &maps.f[k], &bar[s], i0, j0);
+        tma_load_2d(st + 6 * ARR_BYTES, &maps.dvx, &bar[s], i0, j0);
+        tma_load_2d(st + 6 * ARR_BYTES + DV_BYTES, &maps.dvy, &bar[s], i0, j0);
+    };
+    int t = blockIdx.x;
+    if (tid == 0 && t < ntiles) issue(t, 0);
+    uint32_t phase = 0;  // bit s: parity of the next completion of stage s
+    int s = 0;
+    const double dt = *p.dt_ptr;
+    for (; t < ntiles; t += gridDim.x) {
+        const int tn = t + gridDim.x;
+        if (tid == 0 && tn < ntiles) issue(tn, s ^ 1);
+        const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
+        phase ^= 1u << s;
+        if (__syncthreads_or(!ok)) {
+            // a copy never completed: flag it, give in-flight copies a bounded chance to land, leave
+            if (tid == 0) {
+                atomicExch(p.err_flag, 1);
+                mbar_wait(&bar[s], ((phase >> s) & 1u) ^ 1u, WAIT_BUDGET_NS);
+                if (tn < ntiles) mbar_wait(&bar[s ^ 1], (phase >> (s ^ 1)) & 1u, WAIT_BUDGET_NS);
+            }
+            __syncthreads();
+            return;
+        }
+        unsigned char* st = smem + s * STAGE_BYTES;
+        Row2* sVx = reinterpret_cast<Row2*>(st + S_VX * ARR_BYTES);
+        Row2* sVy = reinterpret_cast<Row2*>(st + S_VY * ARR_BYTES);
+        Row2* sRho = reinterpret_cast<Row2*>(st + S_RHO * ARR_BYTES);
+        Row2* sPo = reinterpret_cast<Row2*>(st + S_P * ARR_BYTES);
+        Row2* sMup = reinterpret_cast<Row2*>(st + S_MUP * ARR_BYTES);
+        Row2* sMub = reinterpret_cast<Row2*>(st + S_MUB * ARR_BYTES);
+        RowD* sDvx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES);
+        RowD* sDvy = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + DV_BYTES);
+        const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
 
-    const double _dx = p._dx, _dy = p._dy;
-    // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
-    for (int idx = tid; idx < W1 * H1; idx += NT) {
-        int a = idx % W1, b = idx / W1;
-        int i = i0 + a, j = j0 + b;
-        if (i < Nx - 1 && j < Ny - 1) {
-            double vx1 = sVx[b + 1][a], vx2 = sVx[b + 1][a + 1];
-            double vy1 = sVy[b][a + 1], vy2 = sVy[b + 1][a + 1];
-            double dVx_dx = (vx2 - vx1) * _dx;
-            double dVy_dy = (vy2 - vy1) * _dy;
-            double div_V = dVx_dx + dVy_dy;
-            double mu = sMup[b][a];
-            double dtP = p.c_ptsc * mu / p.max_nxy;       // Ptsc*4.1*mu_p/max_nxy (:131)
-            double Pn = sP[b][a] - dtP * div_V;
-            sP[b][a] = Pn;
-            double txx = 2.0 * mu * (dVx_dx - 1.0 / 3.0 * div_V);
-            double tyy = 2.0 * mu * (dVy_dy - 1.0 / 3.0 * div_V);
-            sTxx[b][a] = txx;
-            sTyy[b][a] = tyy;
-            if (STORE && a < BX && b < BY) {
-                int64_t o = i + (int64_t)j * LD;
-                p.divV[o] = div_V;
-                p.txx[o] = txx;
-                p.tyy[o] = tyy;
+        // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
+        for (int b = ty; b < H1; b += TY) {
+            for (int a = tx; a < W1; a += BX) {
+                const int i = i0 + a, j = j0 + b;
+                if (i < Nx - 1 && j < Ny - 1) {
+                    double vx1 = sVx[b + 1][a], vx2 = sVx[b + 1][a + 1];
+                    double vy1 = sVy[b][a + 1], vy2 = sVy[b + 1][a + 1];
+                    double dVx_dx = (vx2 - vx1) * _dx;
+                    double dVy_dy = (vy2 - vy1) * _dy;
+                    double div_V = dVx_dx + dVy_dy;
+                    double mu = sMup[b][a];
+                    // Ptsc*4.1*mu_p/max_nxy (:131); for a power-of-two max_nxy the product by its
+                    // reciprocal is the same correctly rounded value
+                    double dtP = p.pow2 ? p.c_ptsc * mu * p.inv_max_nxy : p.c_ptsc * mu / p.max_nxy;
+                    sPn[b][a] = sPo[b][a] - dtP * div_V;
+                    double txx = 2.0 * mu * (dVx_dx - 1.0 / 3.0 * div_V);
+                    double tyy = 2.0 * mu * (dVy_dy - 1.0 / 3.0 * div_V);
+                    sTxx[b][a] = txx;
+                    sTyy[b][a] = tyy;
+                    if (STORE && a < BX && b < BY) {
+                        int64_t o = i + (int64_t)j * LD;
+                        p.divV[o] = div_V;
+                        p.txx[o] = txx;
+                        p.tyy[o] = tyy;
+                    }
+                }
+                if (i < Nx && j < Ny) {
+                    double vx0 = sVx[b][a], vx1 = sVx[b + 1][a];
+                    double vy0 = sVy[b][a], vy1 = sVy[b][a + 1];
+                    double dVx_dy = (vx1 - vx0) * _dy;
+                    double dVy_dx = (vy1 - vy0) * _dx;
+                    double tv = 2.0 * sMub[b][a] * 0.5 * (dVx_dy + dVy_dx);
+                    sTxy[b][a] = tv;
+                    if (STORE && (a < BX || i == Nx - 1) && (b < BY || j == Ny - 1)) p.txy[i + (int64_t)j * LD] = tv;
+                }
             }
         }
-        if (i < Nx && j < Ny) {
-            double vx0 = sVx[b][a], vx1 = sVx[b + 1][a];
-            double vy0 = sVy[b][a], vy1 = sVy[b][a + 1];
-            double dVx_dy = (vx1 - vx0) * _dy;
-            double dVy_dx = (vy1 - vy0) * _dx;
-            double t = 2.0 * sTxy[b][a] * 0.5 * (dVx_dy + dVy_dx);
-            sTxy[b][a] = t;
-            if (STORE && (a < BX || i == Nx - 1) && (b < BY || j == Ny - 1)) p.txy[i + (int64_t)j * LD] = t;
-        }
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // ---- stage 2: compute_dV! (:209-219), compute_V! (:226-234), BCs (:53-56) ----
-    const double dt = *p.dt_ptr;
+        // ---- stage 2: compute_dV! (:209-219), compute_V! (:226-234), BCs (:53-56) ----
 #pragma unroll
-    for (int r = 0; r < RPT; ++r) {
-        const int a = threadIdx.x, b = threadIdx.y + r * TY;
-        const int i = i0 + a, j = j0 + b;
-        if (i >= Nx - 1 || j >= Ny - 1) continue;
-        p.P_out[i + (int64_t)j * LD] = sP[b][a];
-        if (i < Nx - 2) {
-            // compute_ResX (:176-182)
-            double Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy
-                        - (sP[b][a + 1] - sP[b][a]) * _dx;
-            double dv = p.dampX * dvx_old[r] + Rx;
-            p.dVx[i + (int64_t)j * LD] = dv;
-            double dtau = p.c_vsc / ((sMup[b][a] + sMup[b][a + 1]) * 0.5) / 4.1;  // :129
-            double vn = sVx[b + 1][a + 1] + dtau * dv;
-            p.Vx_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
-            if (j == 0) p.Vx_out[(i + 1)] = vn;                                   // bc_y_noflux!
-            if (j == Ny - 2) p.Vx_out[(i + 1) + (int64_t)Ny * LD] = vn;
+        for (int r = 0; r < RPT; ++r) {
+            const int a = tx, b = ty + r * TY;
+            const int i = i0 + a, j = j0 + b;
+            if (i >= Nx - 1 || j >= Ny - 1) continue;
+            p.P_out[i + (int64_t)j * LD] = sPn[b][a];
+            if (i < Nx - 2) {
+                // compute_ResX (:176-182)
+                double Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy
+                            - (sPn[b][a + 1] - sPn[b][a]) * _dx;
+                double dv = p.dampX * sDvx[b][a] + Rx;
+                p.dVx[i + (int64_t)j * LD] = dv;
+                double dtau = p.c_vsc / ((sMup[b][a] + sMup[b][a + 1]) * 0.5) / 4.1;  // :129
+                double vn = sVx[b + 1][a + 1] + dtau * dv;
+                p.Vx_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
+                if (j == 0) p.Vx_out[(i + 1)] = vn;                                   // bc_y_noflux!
+                if (j == Ny - 2) p.Vx_out[(i + 1) + (int64_t)Ny * LD] = vn;
+            }
+            if (j < Ny - 2) {
+                // compute_ResY (:189-202)
+                double av_inn_y_Vx = 0.25 * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
+                double d_xi_2_rho = sRho[b + 1][a + 2] - sRho[b + 1][a];
+                double d_yi_2_rho = sRho[b + 2][a + 1] - sRho[b][a + 1];
+                double Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx
+                            - (sPn[b + 1][a] - sPn[b][a]) * _dy
+                            + p.g_y * (sRho[b + 1][a + 1] - dt * (av_inn_y_Vx * d_xi_2_rho * 0.5 * _dx
+                                                                   + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
+                double dv = p.dampY * sDvy[b][a] + Ry;
+                p.dVy[i + (int64_t)j * LD] = dv;
+                double dtau = p.c_vsc / ((sMup[b][a] + sMup[b + 1][a]) * 0.5) / 4.1;  // :130
+                double vn = sVy[b + 1][a + 1] + dtau * dv;
+                p.Vy_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
+                if (i == 0) p.Vy_out[(int64_t)(j + 1) * LD] = vn;                     // bc_x_noflux!
+                if (i == Nx - 2) p.Vy_out[Nx + (int64_t)(j + 1) * LD] = vn;
+            }
+            // constant free-slip entries: bc_x_zero!(Vx) and bc_y_zero!(Vy), corners included
+            if (i == 0 || i == Nx - 2) {
+                int ic = (i == 0) ? 0 : Nx - 1;
+                p.Vx_out[ic + (int64_t)(j + 1) * LD] = 0.0;
+                if (j == 0) p.Vx_out[ic] = 0.0;
+                if (j == Ny - 2) p.Vx_out[ic + (int64_t)Ny * LD] = 0.0;
+            }
+            if (j == 0 || j == Ny - 2) {
+                int64_t jr = (j == 0) ? 0 : (int64_t)(Ny - 1) * LD;
+                p.Vy_out[(i + 1) + jr] = 0.0;
+                if (i == 0) p.Vy_out[jr] = 0.0;
+                if (i == Nx - 2) p.Vy_out[Nx + jr] = 0.0;
+            }
         }
-        if (j < Ny - 2) {
-            // compute_ResY (:189-202)
-            double av_inn_y_Vx = 0.25 * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
-            double d_xi_2_rho = sRho[b + 1][a + 2] - sRho[b + 1][a];
-            double d_yi_2_rho = sRho[b + 2][a + 1] - sRho[b][a + 1];
-            double Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx
-                        - (sP[b + 1][a] - sP[b][a]) * _dy
-                        + p.g_y * (sRho[b + 1][a + 1] - dt * (av_inn_y_Vx * d_xi_2_rho * 0.5 * _dx
-                                                               + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
-            double dv = p.dampY * dvy_old[r] + Ry;
-            p.dVy[i + (int64_t)j * LD] = dv;
-            double dtau = p.c_vsc / ((sMup[b][a] + sMup[b + 1][a]) * 0.5) / 4.1;  // :130
-            double vn = sVy[b + 1][a + 1] + dtau * dv;
-            p.Vy_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
-            if (i == 0) p.Vy_out[(int64_t)(j + 1) * LD] = vn;                     // bc_x_noflux!
-            if (i == Nx - 2) p.Vy_out[Nx + (int64_t)(j + 1) * LD] = vn;
-        }
-        // constant free-slip entries: bc_x_zero!(Vx) and bc_y_zero!(Vy), corners included
-        if (i == 0 || i == Nx - 2) {
-            int ic = (i == 0) ? 0 : Nx - 1;
-            p.Vx_out[ic + (int64_t)(j + 1) * LD] = 0.0;
-            if (j == 0) p.Vx_out[ic] = 0.0;
-            if (j == Ny - 2) p.Vx_out[ic + (int64_t)Ny * LD] = 0.0;
-        }
-        if (j == 0 || j == Ny - 2) {
-            int64_t jr = (j == 0) ? 0 : (int64_t)(Ny - 1) * LD;
-            p.Vy_out[(i + 1) + jr] = 0.0;
-            if (i == 0) p.Vy_out[jr] = 0.0;
-            if (i == Nx - 2) p.Vy_out[Nx + jr] = 0.0;
-        }
+        __syncthreads();  // stage s and the stage-1 arrays are free again
+        s ^= 1;
     }
 }
 
@@ -448,10 +497,34 @@ __global__ void k_sum_partials(const double* __restrict__ partials, int n, doubl
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-constexpr int BX = 32, BY = 16, TY = 8;
-
 static unsigned copy_blocks(sf_ctx* ctx, int64_t n) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)ctx->num_sms * 16));
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_tmap_f64(CUtensorMap* map, const double* base, int64_t ld, int64_t rows, int box_w, int box_h) {
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SF_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p)
+            return fail(SF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = (PFN_encodeTiled)p;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(SF_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
+    return SF_OK;
 }
 
 struct Solver {
@@ -460,27 +533,46 @@ struct Solver {
     Layout L;
     PTParams pt;
     ResParams rp;
-    int cur = 0;  // 0: current V/P in A buffers, 1: in B buffers
+    TmaMaps maps[2];  // [cur]: inputs read from the A (cur = 0) or B (cur = 1) buffers
+    int cur = 0;      // 0: current V/P in A buffers, 1: in B buffers
     int res_blocks = 0;
     int maxv_blocks = 0;
+    int pt_blocks = 0;
     double maxdisp, dx, dy;
 
+    int setup_maps() {
+        const int64_t LD = L.LD, R = L.rows;
+        for (int c = 0; c < 2; ++c) {
+            const int fields[6] = {c ? F_VXB : F_VXA, c ? F_VYB : F_VYA, F_RHO, c ? F_PB : F_PA, F_MUP, F_MUB};
+            for (int k = 0; k < 6; ++k) {
+                int rc = encode_tmap_f64(&maps[c].f[k], L.f(fields[k]), LD, R, TW, TH);
+                if (rc) return rc;
+            }
+            int rc = encode_tmap_f64(&maps[c].dvx, L.f(F_DVX), LD, R, BX, BY);
+            if (!rc) rc = encode_tmap_f64(&maps[c].dvy, L.f(F_DVY), LD, R, BX, BY);
+            if (rc) return rc;
+        }
+        static bool attr_set = false;
+        if (!attr_set) {
+            SF_CUDA(cudaFuncSetAttribute(k_pt_iter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+            SF_CUDA(cudaFuncSetAttribute(k_pt_iter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+            attr_set = true;
+        }
+        pt.ntx = (int)ceil_div(L.Nx - 1, BX);
+        pt.nty = (int)ceil_div(L.Ny - 1, BY);
+        pt_blocks = (int)std::min<int64_t>((int64_t)pt.ntx * pt.nty, 2 * (int64_t)ctx->num_sms);
+        return SF_OK;
+    }
+
     int launch_iter(bool store) {
-        const double* vxi = L.f(cur ? F_VXB : F_VXA);
-        const double* vyi = L.f(cur ? F_VYB : F_VYA);
-        const double* pi = L.f(cur ? F_PB : F_PA);
-        pt.Vx_in = vxi;
-        pt.Vy_in = vyi;
-        pt.P_in = pi;
         pt.Vx_out = L.f(cur ? F_VXA : F_VXB);
         pt.Vy_out = L.f(cur ? F_VYA : F_VYB);
         pt.P_out = L.f(cur ? F_PA : F_PB);
-        dim3 grid((unsigned)ceil_div(L.Nx - 1, BX), (unsigned)ceil_div(L.Ny - 1, BY));
         dim3 block(BX, TY);
         if (store)
-            k_pt_iter<BX, BY, TY, true><<<grid, block, 0, s>>>(pt);
+            k_pt_iter<true><<<pt_blocks, block, SMEM_BYTES, s>>>(maps[cur], pt);
         else
-            k_pt_iter<BX, BY, TY, false><<<grid, block, 0, s>>>(pt);
+            k_pt_iter<false><<<pt_blocks, block, SMEM_BYTES, s>>>(maps[cur], pt);
         SF_LAUNCHED(ctx);
         cur ^= 1;
         return SF_OK;
@@ -629,6 +721,15 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     pt.c_vsc = Vsc * min_dxy2;
     pt.c_ptsc = Ptsc * 4.1;
     pt.max_nxy = max_nxy;
+    {
+        int e = 0;
+        double fr = std::frexp(max_nxy, &e);
+        pt.pow2 = (fr == 0.5) ? 1 : 0;
+        pt.inv_max_nxy = pt.pow2 ? std::ldexp(1.0, 1 - e) : 0.0;
+    }
+    pt.err_flag = ctx->d_flags;
+    SF_CUDA(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), s));
+    if ((rc = S.setup_maps())) return rc;
     ResParams& rp = S.rp;
     rp.txx = S.L.f(F_TXX);
     rp.tyy = S.L.f(F_TYY);
@@ -740,6 +841,9 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
         info->fused_launches = fused;
         info->fused_ms = 0.0;
     }
+    int hflag = 0;
+    SF_CUDA(cudaMemcpy(&hflag, ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hflag) return fail(SF_ERR_CUDA, "sf_solve_stokes: a tile copy into shared memory did not complete in time");
     if (!(err == err) || std::isinf(err)) return fail(SF_ERR_NONFINITE, "sf_solve_stokes: residual is not finite");
     return SF_OK;
 }
