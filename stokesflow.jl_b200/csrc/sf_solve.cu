@@ -46,7 +46,7 @@ namespace sf {
 
 enum {
     F_VXA, F_VXB, F_VYA, F_VYB, F_PA, F_PB, F_DVX, F_DVY, F_RHO, F_MUB, F_MUP,
-    F_TXX, F_TYY, F_TXY, F_DIV, F_RX, F_RY, F_NUM
+    F_TXX, F_TYY, F_TXY, F_DIV, F_RX, F_RY, F_DTVX, F_DTVY, F_NUM
 };
 
 struct Layout {
@@ -93,26 +93,36 @@ struct PTParams {
 // overlap the arithmetic without needing high occupancy.  A stage holds the
 // old Vx, Vy, rho_vy, P, mu_p, mu_b boxes (tile + 2 halo; the TMA zero-fills
 // beyond the arrays) and the dVx, dVy boxes (tile only).
-constexpr int BX = 32, BY = 16, TY = 8;      // owned tile, threads (BX x TY)
+#ifndef SF_PT_BY
+#define SF_PT_BY 16
+#endif
+#ifndef SF_PT_TY
+#define SF_PT_TY 8
+#endif
+constexpr int BX = 32, BY = SF_PT_BY, TY = SF_PT_TY;   // owned tile, threads (BX x TY)
+static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
+constexpr int PT_THREADS = BX * TY;
+constexpr int PT_MIN_BLOCKS = (PT_THREADS >= 512) ? 2 : 3;
 constexpr int TW = BX + 2, TH = BY + 2;      // staged box (tile + 2 halo); TW*8 is a multiple of 16 bytes
 constexpr int W1 = BX + 1, H1 = BY + 1;      // P / tau points computed per tile (tile + 1 halo)
 constexpr int RPT = BY / TY;                 // owned rows per thread
 constexpr int ARR_BYTES = ((TH * TW * 8 + 127) / 128) * 128;
 constexpr int DV_BYTES = ((BY * BX * 8 + 127) / 128) * 128;
 constexpr int ST1_BYTES = ((H1 * W1 * 8 + 127) / 128) * 128;
-constexpr int STAGE_BYTES = 6 * ARR_BYTES + 2 * DV_BYTES;
-constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 2 * BY * BX * 8;  // bytes delivered per stage
+constexpr int STAGE_BYTES = 6 * ARR_BYTES + 4 * DV_BYTES;         // + dVx, dVy, dtauVx, dtauVy boxes
+constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 4 * BY * BX * 8;  // bytes delivered per stage
 constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 4 * ST1_BYTES + 64;
 constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;                 // 2 s per stage wait
 enum { S_VX = 0, S_VY, S_RHO, S_P, S_MUP, S_MUB };
 
 struct TmaMaps {
     CUtensorMap f[6];  // S_* order
-    CUtensorMap dvx, dvy;
+    CUtensorMap dvx, dvy, dtx, dty;
 };
 
 template <bool STORE>
-__global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ TmaMaps maps, PTParams p) {
+__global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __grid_constant__ TmaMaps maps,
+                                                                      PTParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     typedef double Row1[W1];
     typedef double Row2[TW];
@@ -142,6 +152,8 @@ __global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ 
         for (int k = 0; k < 6; ++k) tma_load_2d(st + k * ARR_BYTES, &maps.f[k], &bar[s], i0, j0);
         tma_load_2d(st + 6 * ARR_BYTES, &maps.dvx, &bar[s], i0, j0);
         tma_load_2d(st + 6 * ARR_BYTES + DV_BYTES, &maps.dvy, &bar[s], i0, j0);
+        tma_load_2d(st + 6 * ARR_BYTES + 2 * DV_BYTES, &maps.dtx, &bar[s], i0, j0);
+        tma_load_2d(st + 6 * ARR_BYTES + 3 * DV_BYTES, &maps.dty, &bar[s], i0, j0);
     };
     int t = blockIdx.x;
     if (tid == 0 && t < ntiles) issue(t, 0);
@@ -172,6 +184,8 @@ __global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ 
         Row2* sMub = reinterpret_cast<Row2*>(st + S_MUB * ARR_BYTES);
         RowD* sDvx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES);
         RowD* sDvy = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + DV_BYTES);
+        RowD* sDtx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 2 * DV_BYTES);  // dtauVx of :129
+        RowD* sDty = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 3 * DV_BYTES);  // dtauVy of :130
         const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
 
         // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
@@ -226,8 +240,7 @@ __global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ 
                             - (sPn[b][a + 1] - sPn[b][a]) * _dx;
                 double dv = p.dampX * sDvx[b][a] + Rx;
                 p.dVx[i + (int64_t)j * LD] = dv;
-                double dtau = p.c_vsc / ((sMup[b][a] + sMup[b][a + 1]) * 0.5) / 4.1;  // :129
-                double vn = sVx[b + 1][a + 1] + dtau * dv;
+                double vn = sVx[b + 1][a + 1] + sDtx[b][a] * dv;
                 p.Vx_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
                 if (j == 0) p.Vx_out[(i + 1)] = vn;                                   // bc_y_noflux!
                 if (j == Ny - 2) p.Vx_out[(i + 1) + (int64_t)Ny * LD] = vn;
@@ -243,8 +256,7 @@ __global__ void __launch_bounds__(BX * TY, 2) k_pt_iter(const __grid_constant__ 
                                                                    + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
                 double dv = p.dampY * sDvy[b][a] + Ry;
                 p.dVy[i + (int64_t)j * LD] = dv;
-                double dtau = p.c_vsc / ((sMup[b][a] + sMup[b + 1][a]) * 0.5) / 4.1;  // :130
-                double vn = sVy[b + 1][a + 1] + dtau * dv;
+                double vn = sVy[b + 1][a + 1] + sDty[b][a] * dv;
                 p.Vy_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
                 if (i == 0) p.Vy_out[(int64_t)(j + 1) * LD] = vn;                     // bc_x_noflux!
                 if (i == Nx - 2) p.Vy_out[Nx + (int64_t)(j + 1) * LD] = vn;
@@ -459,17 +471,18 @@ __global__ void k_pad_vy(double* __restrict__ pad, const double* __restrict__ Vy
     }
 }
 
-// compute_timesteps! (:128-133) into the caller's dtVx (Nx-2,Ny-1), dtVy (Nx-1,Ny-2), dtPt (Nx-1,Ny-1)
+// compute_timesteps! (:128-133): dtVx (Nx-2,Ny-1), dtVy (Nx-1,Ny-2), dtPt (Nx-1,Ny-1) with leading
+// dimensions ld_x, ld_y, ld_p (the caller's dense arrays, or the padded internal ones); NULL skips one
 __global__ void k_timesteps(const double* __restrict__ mup, int64_t LD, int Nx, int Ny, double c_vsc, double c_ptsc,
-                            double max_nxy, double* __restrict__ dtVx, double* __restrict__ dtVy,
-                            double* __restrict__ dtPt) {
+                            double max_nxy, double* __restrict__ dtVx, int64_t ld_x, double* __restrict__ dtVy,
+                            int64_t ld_y, double* __restrict__ dtPt, int64_t ld_p) {
     int64_t W = Nx - 1, n = W * (Ny - 1);
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
         int i = (int)(k % W), j = (int)(k / W);
         int64_t o = i + (int64_t)j * LD;
-        if (dtVx && i < Nx - 2) dtVx[i + (int64_t)j * (Nx - 2)] = c_vsc / ((mup[o] + mup[o + 1]) * 0.5) / 4.1;
-        if (dtVy && j < Ny - 2) dtVy[i + (int64_t)j * (Nx - 1)] = c_vsc / ((mup[o] + mup[o + LD]) * 0.5) / 4.1;
-        if (dtPt) dtPt[k] = c_ptsc * mup[o] / max_nxy;
+        if (dtVx && i < Nx - 2) dtVx[i + (int64_t)j * ld_x] = c_vsc / ((mup[o] + mup[o + 1]) * 0.5) / 4.1;
+        if (dtVy && j < Ny - 2) dtVy[i + (int64_t)j * ld_y] = c_vsc / ((mup[o] + mup[o + LD]) * 0.5) / 4.1;
+        if (dtPt) dtPt[i + (int64_t)j * ld_p] = c_ptsc * mup[o] / max_nxy;
     }
 }
 
@@ -550,6 +563,8 @@ struct Solver {
             }
             int rc = encode_tmap_f64(&maps[c].dvx, L.f(F_DVX), LD, R, BX, BY);
             if (!rc) rc = encode_tmap_f64(&maps[c].dvy, L.f(F_DVY), LD, R, BX, BY);
+            if (!rc) rc = encode_tmap_f64(&maps[c].dtx, L.f(F_DTVX), LD, R, BX, BY);
+            if (!rc) rc = encode_tmap_f64(&maps[c].dty, L.f(F_DTVY), LD, R, BX, BY);
             if (rc) return rc;
         }
         static bool attr_set = false;
@@ -558,9 +573,14 @@ struct Solver {
             SF_CUDA(cudaFuncSetAttribute(k_pt_iter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
             attr_set = true;
         }
+        static int per_sm = 0;
+        if (!per_sm) {
+            SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt_iter<false>, PT_THREADS, SMEM_BYTES));
+            if (per_sm < 1) return fail(SF_ERR_CUDA, "k_pt_iter does not fit on an SM");
+        }
         pt.ntx = (int)ceil_div(L.Nx - 1, BX);
         pt.nty = (int)ceil_div(L.Ny - 1, BY);
-        pt_blocks = (int)std::min<int64_t>((int64_t)pt.ntx * pt.nty, 2 * (int64_t)ctx->num_sms);
+        pt_blocks = (int)std::min<int64_t>((int64_t)pt.ntx * pt.nty, (int64_t)per_sm * ctx->num_sms);
         return SF_OK;
     }
 
@@ -692,10 +712,17 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     }
     k_set_scalar<<<1, 1, 0, s>>>(ctx->d_scalars + SC_DT, dt);
     SF_LAUNCHED(ctx);
+    // compute_timesteps! (:34): dtauVx, dtauVy once per solve into the padded layout (the fused
+    // kernel reads them instead of dividing every iteration); also into the caller's arrays if given
+    k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
+                                                                     Vsc * min_dxy2, Ptsc * 4.1, max_nxy,
+                                                                     S.L.f(F_DTVX), LD, S.L.f(F_DTVY), LD,
+                                                                     nullptr, 0);
+    SF_LAUNCHED(ctx);
     if (dtVx || dtVy || dtPt) {
         k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
                                                                          Vsc * min_dxy2, Ptsc * 4.1, max_nxy, dtVx,
-                                                                         dtVy, dtPt);
+                                                                         Nx - 2, dtVy, Nx - 1, dtPt, Nx - 1);
         SF_LAUNCHED(ctx);
     }
 
