@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--n", type=int, default=2048, help="grid points per side (cells = n - 1)")
     ap.add_argument("--markers-per-cell", type=int, default=16)
     ap.add_argument("--rtol", type=float, default=1e-6)
-    ap.add_argument("--iter-max", type=int, default=100000, help="reference default iterMax")
+    ap.add_argument("--iter-max", type=int, default=400000,
+                    help="PT iteration cap per solve (reference default 100000; a cold 2048^2 start needs ~250k)")
     ap.add_argument("--mu-air", type=float, default=1e-2,
                     help="air viscosity; 1e-3 makes the reference PT scheme diverge (see DESIGN.md)")
     ap.add_argument("--no-e2e", action="store_true")
