@@ -90,6 +90,28 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
                                double* val_wt_sum, double* wt_sum, int64_t ld_sum, int64_t n_sum,
                                void* stream);
 
+/* Allocation-free deposit.  No counterpart in the reference: it is
+ * sf_bilinear_marker_to_grid (same result, bit for bit) for callers that cannot
+ * let a library allocate device memory -- a host runtime that owns the GPU
+ * memory through its own pool, a latency-critical stream loop that cudaMalloc /
+ * cudaFree would stall with their device-wide synchronisation, a process held
+ * to a fixed memory budget.  It takes no context and allocates nothing: its
+ * scratch is a fixed array inside the library (about 11 MB, held on every GPU
+ * that loads the library until the process exits), so it accepts at most
+ * SF_NOALLOC_MAX_MARKERS markers and grids with (nx+1)*(ny+1) <=
+ * SF_NOALLOC_MAX_CELLS, and returns SF_ERR_TOO_LARGE beyond that.  It runs on
+ * the calling thread's current device.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and caches it; make that
+ * first call before any stream capture.  All calls share the one array, so
+ * calls whose work overlaps on the GPU (different streams, or different host
+ * threads on the same device) race and must be serialised by the caller.
+ * Warning counts are not reported.  val_wt_sum / wt_sum are not produced. */
+#define SF_NOALLOC_MAX_MARKERS 1048576
+#define SF_NOALLOC_MAX_CELLS 262144
+int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_grid_min, double* val_grid, int64_t nx,
+                                       int64_t ny, const double* x_m, const double* y_m, const double* val_m,
+                                       int64_t nm, double dx, double dy, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* pseudo-transient Stokes solve                                             */
 /* ---------------------------------------------------------------------- */

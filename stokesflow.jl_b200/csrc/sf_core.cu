@@ -152,6 +152,23 @@ int exclusive_scan_i32(sf_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, 
     return SF_OK;
 }
 
+// Same scan with the caller's tile buffer (ceil(n / 8192) ints); allocates nothing.
+int exclusive_scan_i32_into(const int32_t* in, int32_t* out, int64_t n, int32_t* d_total, int32_t* tiles,
+                            cudaStream_t stream) {
+    int64_t ntiles = ceil_div(n, SCAN_TILE);
+    if (ntiles == 0) {
+        if (d_total) SF_CUDA(cudaMemsetAsync(d_total, 0, sizeof(int32_t), stream));
+        return SF_OK;
+    }
+    k_scan_tile_sums<<<(unsigned)ntiles, SCAN_THREADS, 0, stream>>>(in, n, tiles);
+    SF_CHECK_LAUNCH();
+    k_scan_tile_offsets<<<1, SCAN_THREADS, 0, stream>>>(tiles, ntiles, d_total);
+    SF_CHECK_LAUNCH();
+    k_scan_tiles<<<(unsigned)ntiles, SCAN_THREADS, 0, stream>>>(in, out, n, tiles);
+    SF_CHECK_LAUNCH();
+    return SF_OK;
+}
+
 // --------------------------------------------------------------------------
 // marker initialisation, scripts/common.jl:40-110 (single rank)
 // --------------------------------------------------------------------------

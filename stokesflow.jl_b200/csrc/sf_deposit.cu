@@ -245,3 +245,111 @@ int sf_rebin_markers(sf_ctx* ctx, const double* x_m, const double* y_m, int64_t 
 }
 
 }  // extern "C"
+
+// ==========================================================================
+// Allocation-free deposit
+// ==========================================================================
+// Some callers cannot let a library call cudaMalloc / cudaFree: hosts whose
+// runtime owns the device memory through its own pool (for example Julia's
+// CUDA.jl or PyTorch with the rest of the GPU reserved), where an allocation
+// outside the pool fails or forces an eviction; latency-critical stream loops,
+// where cudaMalloc / cudaFree synchronise the whole device and stall the other
+// streams; and processes held to a fixed memory budget after start-up.  For
+// them sf_bilinear_marker_to_grid_noalloc runs the same deposit with all of
+// its scratch in the file-scope array below, which every GPU that loads the
+// library holds (about 11 MB) until the process exits.
+#include <mutex>
+
+namespace sf {
+
+constexpr int64_t NA_MAX_MARKERS = SF_NOALLOC_MAX_MARKERS;
+constexpr int64_t NA_MAX_CELLS = SF_NOALLOC_MAX_CELLS;          // (nx + 1) * (ny + 1)
+constexpr int64_t NA_SCAN_TILES = (NA_MAX_CELLS + 1 + 8191) / 8192;
+// layout (bytes): keys | perm | counts | offsets | cursor | scan tiles | counters
+constexpr size_t NA_OFF_KEYS = 0;
+constexpr size_t NA_OFF_PERM = NA_OFF_KEYS + 4 * NA_MAX_MARKERS;
+constexpr size_t NA_OFF_COUNTS = NA_OFF_PERM + 4 * NA_MAX_MARKERS;
+constexpr size_t NA_OFF_OFFSETS = NA_OFF_COUNTS + 4 * (NA_MAX_CELLS + 64);
+constexpr size_t NA_OFF_CURSOR = NA_OFF_OFFSETS + 4 * (NA_MAX_CELLS + 64);
+constexpr size_t NA_OFF_TILES = NA_OFF_CURSOR + 4 * (NA_MAX_CELLS + 64);
+constexpr size_t NA_OFF_COUNTERS = NA_OFF_TILES + 4 * ((NA_SCAN_TILES + 63) / 64 * 64);
+constexpr size_t NA_BYTES = NA_OFF_COUNTERS + 2 * sizeof(unsigned long long);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+static unsigned char* g_noalloc_ptr[NA_MAX_DEVICES] = {};
+static std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached.
+static int noalloc_scratch(unsigned char** out) {
+    int dev = 0;
+    SF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(SF_ERR_NO_DEVICE, "noalloc deposit: device index too large");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            (void)cudaGetLastError();
+            return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
+        }
+        g_noalloc_ptr[dev] = (unsigned char*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return SF_OK;
+}
+
+}  // namespace sf
+
+extern "C" int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_grid_min, double* val_grid, int64_t nx,
+                                                  int64_t ny, const double* x_m, const double* y_m, const double* val_m,
+                                                  int64_t nm, double dx, double dy, void* stream) {
+    SF_REQUIRE(val_grid && nx >= 1 && ny >= 1, "sf_bilinear_marker_to_grid_noalloc: bad grid");
+    SF_REQUIRE(nm >= 0 && (nm == 0 || (x_m && y_m && val_m)), "sf_bilinear_marker_to_grid_noalloc: bad markers");
+    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_bilinear_marker_to_grid_noalloc: dx, dy must be positive");
+    if (nm > NA_MAX_MARKERS)
+        return fail(SF_ERR_TOO_LARGE, "sf_bilinear_marker_to_grid_noalloc: " + std::to_string(nm) +
+                                          " markers exceed the fixed scratch (at most " +
+                                          std::to_string(NA_MAX_MARKERS) + ")");
+    if (nx > NA_MAX_CELLS || ny > NA_MAX_CELLS || (nx + 1) * (ny + 1) > NA_MAX_CELLS)
+        return fail(SF_ERR_TOO_LARGE, "sf_bilinear_marker_to_grid_noalloc: a " + std::to_string(nx) + " x " +
+                                          std::to_string(ny) + " grid exceeds the fixed scratch (at most " +
+                                          std::to_string(NA_MAX_CELLS) + " cells (nx+1)*(ny+1))");
+    unsigned char* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    int32_t* keys = (int32_t*)(base + NA_OFF_KEYS);
+    int32_t* perm = (int32_t*)(base + NA_OFF_PERM);
+    int32_t* counts = (int32_t*)(base + NA_OFF_COUNTS);
+    int32_t* offsets = (int32_t*)(base + NA_OFF_OFFSETS);
+    int32_t* cursor = (int32_t*)(base + NA_OFF_CURSOR);
+    int32_t* tiles = (int32_t*)(base + NA_OFF_TILES);
+    unsigned long long* counters = (unsigned long long*)(base + NA_OFF_COUNTERS);
+    const int64_t ncells = (nx + 1) * (ny + 1);
+    // the array keeps the previous call's contents: clear what must start at zero
+    SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
+    SF_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(ncells + 1) * 4, s));
+    SF_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s));
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nm, DEP_THREADS), 148 * 32));
+    if (nm > 0) {
+        k_cell_keys<<<blocks, DEP_THREADS, 0, s>>>(x_m, y_m, nm, x_grid_min, y_grid_min, dx, dy, nx, ny, keys, counts,
+                                                   counters + 0);
+        SF_CHECK_LAUNCH();
+    }
+    if ((rc = exclusive_scan_i32_into(counts, offsets, ncells, offsets + ncells, tiles, s))) return rc;
+    if (nm > 0) {
+        k_scatter<<<blocks, DEP_THREADS, 0, s>>>(keys, nm, offsets, cursor, perm);
+        SF_CHECK_LAUNCH();
+    }
+    k_sort_segments<<<(unsigned)ceil_div(ncells, 128), 128, 0, s>>>(offsets, ncells, perm);
+    SF_CHECK_LAUNCH();
+    k_gather<<<(unsigned)ceil_div(nx * ny, DEP_THREADS), DEP_THREADS, 0, s>>>(
+        x_m, y_m, val_m, offsets, perm, nx, ny, x_grid_min, y_grid_min, dx, dy, val_grid, nullptr, nullptr, 0,
+        counters + 1);
+    SF_CHECK_LAUNCH();
+    return SF_OK;
+}

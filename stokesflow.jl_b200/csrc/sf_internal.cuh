@@ -89,6 +89,9 @@ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 // exclusive scan of n int32 values (in may alias out); total -> *d_total (device)
 int exclusive_scan_i32(sf_ctx* ctx, const int32_t* in, int32_t* out, int64_t n, int32_t* d_total,
                        cudaStream_t stream);
+// the same with a caller-provided tile buffer of ceil(n / 8192) ints; allocates nothing
+int exclusive_scan_i32_into(const int32_t* in, int32_t* out, int64_t n, int32_t* d_total, int32_t* tiles,
+                            cudaStream_t stream);
 
 // --------------------------------------------------------------------------
 // device helpers

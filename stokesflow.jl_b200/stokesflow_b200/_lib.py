@@ -22,6 +22,10 @@ SF_ERR_NO_DEVICE = 4
 SF_ERR_NONFINITE = 5
 SF_ERR_TOO_LARGE = 6
 
+# limits of the allocation-free deposit (include/stokesflow_b200.h)
+SF_NOALLOC_MAX_MARKERS = 1048576
+SF_NOALLOC_MAX_CELLS = 262144
+
 _d = C.c_double
 _i64 = C.c_int64
 _i32 = C.c_int32
@@ -65,6 +69,7 @@ PROTOTYPES = {
     "sf_get_warnings": (C.c_int, [_vp, C.POINTER(Warnings), C.c_int]),
     "sf_bilinear_marker_to_grid": (C.c_int, [_vp, _d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _pd, _pd,
                                              _i64, _i64, _vp]),
+    "sf_bilinear_marker_to_grid_noalloc": (C.c_int, [_d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _vp]),
     "sf_solve_stokes": (C.c_int, [_vp] + [_pd] * 19 + [_d, _d, _d, _i64, _i64, _d, _d, C.c_int, _d, C.c_int, _i64,
                                                        _vp, C.POINTER(SolveInfo)]),
     "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),

@@ -150,6 +150,23 @@ def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, d
           "bilinear_marker_to_grid")
 
 
+def bilinear_marker_to_grid_noalloc(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, dx, dy, *, stream=None):
+    """The deposit of :func:`bilinear_marker_to_grid` without any device allocation, for callers that
+    cannot let a library allocate GPU memory (a runtime that owns the memory through its own pool, a
+    stream loop that cudaMalloc's device-wide synchronisation would stall, a fixed memory budget).
+    Scratch is a fixed array inside the library, so at most SF_NOALLOC_MAX_MARKERS markers and
+    (nx+1)*(ny+1) <= SF_NOALLOC_MAX_CELLS; calls that overlap on the GPU race (they share that array).
+    Runs on the current device; no context is used."""
+    nx, ny = val_grid.shape
+    nm = x_m.numel()
+    if y_m.numel() != nm or val_m.numel() != nm:
+        raise ValueError("x_m, y_m, val_m must have the same length")
+    check(lib().sf_bilinear_marker_to_grid_noalloc(float(x_grid_min), float(y_grid_min), _grid(val_grid, "val_grid"),
+                                                   nx, ny, _vec(x_m, "x_m"), _vec(y_m, "y_m"), _vec(val_m, "val_m"),
+                                                   nm, float(dx), float(dy), _stream(stream)),
+          "bilinear_marker_to_grid_noalloc")
+
+
 def solve_stokes_info(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt, dtVx,
                       dtVy, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp, comm=None, *,
                       use_free_surface_stabilization=True, eps=1e-8, print_info=False, iter_max=100000,
