@@ -99,7 +99,12 @@ struct PTParams {
 #ifndef SF_PT_TY
 #define SF_PT_TY 8
 #endif
+#ifndef SF_PT_STAGES
+#define SF_PT_STAGES 2
+#endif
 constexpr int BX = 32, BY = SF_PT_BY, TY = SF_PT_TY;   // owned tile, threads (BX x TY)
+constexpr int NST = SF_PT_STAGES;                      // shared-memory stages (tiles in flight + 1)
+static_assert(NST >= 2 && NST <= 8, "2..8 pipeline stages");
 static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
 constexpr int PT_THREADS = BX * TY;
 constexpr int PT_MIN_BLOCKS = (PT_THREADS >= 512) ? 2 : 3;
@@ -111,7 +116,7 @@ constexpr int DV_BYTES = ((BY * BX * 8 + 127) / 128) * 128;
 constexpr int ST1_BYTES = ((H1 * W1 * 8 + 127) / 128) * 128;
 constexpr int STAGE_BYTES = 6 * ARR_BYTES + 4 * DV_BYTES;         // + dVx, dVy, dtauVx, dtauVy boxes
 constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 4 * BY * BX * 8;  // bytes delivered per stage
-constexpr int SMEM_BYTES = 2 * STAGE_BYTES + 4 * ST1_BYTES + 64;
+constexpr int SMEM_BYTES = NST * STAGE_BYTES + 4 * ST1_BYTES + 64;
 constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;                 // 2 s per stage wait
 enum { S_VX = 0, S_VY, S_RHO, S_P, S_MUP, S_MUB };
 
@@ -127,11 +132,11 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
     typedef double Row1[W1];
     typedef double Row2[TW];
     typedef double RowD[BX];
-    Row1* sPn = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES);
-    Row1* sTxx = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + ST1_BYTES);
-    Row1* sTyy = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + 2 * ST1_BYTES);
-    Row1* sTxy = reinterpret_cast<Row1*>(smem + 2 * STAGE_BYTES + 3 * ST1_BYTES);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * STAGE_BYTES + 4 * ST1_BYTES);
+    Row1* sPn = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES);
+    Row1* sTxx = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + ST1_BYTES);
+    Row1* sTyy = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + 2 * ST1_BYTES);
+    Row1* sTxy = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + 3 * ST1_BYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NST * STAGE_BYTES + 4 * ST1_BYTES);
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
     const int Nx = p.Nx, Ny = p.Ny, ntiles = p.ntx * p.nty;
@@ -139,8 +144,7 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
     const double _dx = p._dx, _dy = p._dy;
 
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int k = 0; k < NST; ++k) mbar_init(&bar[k], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -155,22 +159,31 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         tma_load_2d(st + 6 * ARR_BYTES + 2 * DV_BYTES, &maps.dtx, &bar[s], i0, j0);
         tma_load_2d(st + 6 * ARR_BYTES + 3 * DV_BYTES, &maps.dty, &bar[s], i0, j0);
     };
+    const int G = gridDim.x;
     int t = blockIdx.x;
-    if (tid == 0 && t < ntiles) issue(t, 0);
+    // prologue: the first NST-1 tiles of this CTA into stages 0 .. NST-2
+    if (tid == 0)
+        for (int k = 0; k < NST - 1; ++k)
+            if (t + k * G < ntiles) issue(t + k * G, k);
     uint32_t phase = 0;  // bit s: parity of the next completion of stage s
     int s = 0;
     const double dt = *p.dt_ptr;
-    for (; t < ntiles; t += gridDim.x) {
-        const int tn = t + gridDim.x;
-        if (tid == 0 && tn < ntiles) issue(tn, s ^ 1);
+    for (; t < ntiles; t += G) {
+        // refill the stage freed by the previous tile with the tile NST-1 ahead
+        const int tn = t + (NST - 1) * G;
+        if (tid == 0 && tn < ntiles) issue(tn, (s + NST - 1) % NST);
         const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
         phase ^= 1u << s;
         if (__syncthreads_or(!ok)) {
-            // a copy never completed: flag it, give in-flight copies a bounded chance to land, leave
+            // a copy never completed: flag it, give every copy still in flight a bounded chance to land, leave
             if (tid == 0) {
                 atomicExch(p.err_flag, 1);
-                mbar_wait(&bar[s], ((phase >> s) & 1u) ^ 1u, WAIT_BUDGET_NS);
-                if (tn < ntiles) mbar_wait(&bar[s ^ 1], (phase >> (s ^ 1)) & 1u, WAIT_BUDGET_NS);
+                for (int k = 0; k < NST; ++k) {
+                    if (t + k * G >= ntiles) break;
+                    const int sk = (s + k) % NST;
+                    const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
+                    mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
+                }
             }
             __syncthreads();
             return;
@@ -189,8 +202,10 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
 
         // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
-        for (int b = ty; b < H1; b += TY) {
-            for (int a = tx; a < W1; a += BX) {
+        // the (BX+1) x (BY+1) points are spread evenly over all threads, row by row
+        for (int idx = tid; idx < W1 * H1; idx += PT_THREADS) {
+            {
+                const int b = idx / W1, a = idx - b * W1;
                 const int i = i0 + a, j = j0 + b;
                 if (i < Nx - 1 && j < Ny - 1) {
                     double vx1 = sVx[b + 1][a], vx2 = sVx[b + 1][a + 1];
@@ -276,7 +291,7 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
             }
         }
         __syncthreads();  // stage s and the stage-1 arrays are free again
-        s ^= 1;
+        s = (s + 1 == NST) ? 0 : s + 1;
     }
 }
 

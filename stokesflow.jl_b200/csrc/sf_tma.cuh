@@ -49,12 +49,13 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 }
 
 // Wait for phase `parity` of `bar` for at most budget_ns; false on timeout.
+// The clock is read only every 256 polls so that waiting warps stay cheap.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64_t budget_ns) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
-    while (true) {
+    for (uint32_t k = 1;; ++k) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_timer_ns() - t0 > budget_ns) return false;
+        if ((k & 255u) == 0u && global_timer_ns() - t0 > budget_ns) return false;
     }
 }
 
