@@ -44,6 +44,7 @@ METRIC = "PT T_eff (essential HBM bytes of the PT iterations / time), FP64, rela
 UNIT = "GB/s"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+TRAFFIC_PER_LAUNCH_2048 = 469.078e6   # dram__bytes_read.sum + dram__bytes_write.sum, k_pt_iter, 2047^2 points
 
 
 # ---------------------------------------------------------------------------
@@ -63,7 +64,33 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=12, help="PT iterations in the CPU baseline sample")
+    ap.add_argument("--pt-probe", type=int, default=0, metavar="ITERS",
+                    help="kernel probe: run ITERS fused PT iterations of an n x n solve (smooth random fields, no "
+                         "markers) and print the kernel time; used for ncu captures")
     return ap.parse_args()
+
+
+def pt_probe(a):
+    """Fused PT iteration alone: ITERS iterations (no residual check falls inside when ITERS < 2000)."""
+    import stokesflow_b200 as sf
+    n, iters = a.n, a.pt_probe
+    z = sf.zeros
+    P, Vx, Vy = z(n - 1, n - 1), z(n + 2, n + 1), z(n + 1, n + 2)
+    rho, mub, mup = z(n + 1, n), z(n, n), z(n - 1, n - 1)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for arr in (rho, mub, mup):
+        arr.copy_(1.0 + 0.5 * torch.rand(arr.shape[1], arr.shape[0], device="cuda", dtype=torch.float64,
+                                         generator=g).t())
+    dVx, dVy, Vxs, Vys = z(n - 2, n - 1), z(n - 1, n - 2), z(n, n + 1), z(n + 1, n)
+    info = sf.solve_stokes_info(P, Vx, Vy, rho, mub, mup, None, None, None, None, None, None, None, dVx, dVy, None,
+                                None, Vxs, Vys, 9.81, 1 / (n - 1), 1 / (n - 1), n, n, 0.0, 0.5, eps=1e-300,
+                                iter_max=iters)
+    peak, src = peak_hbm()
+    us = info["loop_ms"] * 1e3 / iters
+    gbs = info["bytes_per_iter"] / (us * 1e-6) / 1e9
+    print(json.dumps({"probe": "k_pt_iter", "n": n, "iters": iters, "us_per_iter": round(us, 3),
+                      "t_eff_gbs": round(gbs, 1), "frac_of_peak": round(gbs / peak, 4), "peak_source": src,
+                      "bytes_per_iter": info["bytes_per_iter"]}), flush=True)
 
 
 def bench_config(a):
@@ -208,10 +235,14 @@ def run_ours(a, rank, world, local_rank):
     out["ms_per_timestep"] = {k: round(sum(getattr(r["times"], k) for r in recs) / len(recs), 3)
                               for k in ("deposit_ms", "solve_ms", "advect_ms", "rebin_ms")}
     achieved = bytes_local / (loop_ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) of one k_pt_iter launch from the ncu capture in
+    # profiles/k_pt_iter_plume2048.md (2047^2 points), scaled by the point count
+    traffic = TRAFFIC_PER_LAUNCH_2048 * ((a.n - 1) / 2047.0) ** 2
     out["roofline"] = {"bound": "hbm", "kernel": "k_pt_iter (fused PT iteration)", "achieved": round(achieved, 1),
                        "peak": peak, "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                       "traffic": None, "note": "bytes_per_iter x iterations / PT-loop device time (checks and dt "
-                                                "updates included, pack/unpack excluded)"}
+                       "traffic": round(traffic), "algorithmic_bytes_per_launch": bpi,
+                       "note": "achieved = bytes_per_iter x iterations / PT-loop device time (CUDA events; checks and "
+                               "dt updates included, pack/unpack excluded); traffic from ncu per launch"}
     out["clocks"] = clk
     out["gpu_launches"] = launches
     # ---- end to end through the public API with host buffers ----
@@ -324,6 +355,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.pt_probe:
+        torch.cuda.set_device(local_rank)
+        pt_probe(a)
+        return
     if a.impl == "reference":
         out = run_reference(a, rank)
         if out is not None:
