@@ -161,6 +161,70 @@ int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int6
                              double g_y, void* stream, double* scale);
 
 /* ---------------------------------------------------------------------- */
+/* mixed-precision and batched solves (no reference counterpart: the       */
+/* reference has only the FP64 solveStokes!)                                */
+/* ---------------------------------------------------------------------- */
+/* One Stokes problem of a batch: the caller arrays of sf_solve_stokes
+ * (state in/out, work arrays not needed) plus its scalars; the results are
+ * written back into the struct. */
+typedef struct {
+    double* P;                 /* (Nx-1, Ny-1)  in/out */
+    double* Vx_pad;            /* (Nx+2, Ny+1)  out    */
+    double* Vy_pad;            /* (Nx+1, Ny+2)  out    */
+    const double* rho_vy;      /* (Nx+1, Ny)           */
+    const double* mu_b;        /* (Nx,   Ny)           */
+    const double* mu_p;        /* (Nx-1, Ny-1)         */
+    double* Vx_s;              /* (Nx,   Ny+1)  in/out */
+    double* Vy_s;              /* (Nx+1, Ny)    in/out */
+    int64_t Nx, Ny;
+    double g_y, dx, dy;
+    double dt;                 /* stabilisation dt the solve starts with (the previous timestep's) */
+    double maxdisp;
+    double eps;                /* absolute stopping tolerance, as solveStokes!'s eps          */
+    double rel_tol;            /* if > 0: eps = rel_tol * mean|g_y rho_vy| (relative residual) */
+    int32_t use_free_surface_stabilization;
+    int32_t reserved0;
+    /* results */
+    double dt_out;             /* compute_dt of the final velocities */
+    double err;                /* final FP64 residual norm           */
+    double eps_used;
+    int64_t inner_iters;       /* FP32 PT sweeps                     */
+    int64_t outer_iters;       /* FP64 residual evaluations          */
+    int32_t converged;
+    int32_t status;            /* sf_status of this instance         */
+    double batch_ms;           /* device time of the whole batch     */
+} sf_batch_instance;
+
+typedef struct {
+    int64_t max_sweeps;        /* FP32 sweeps per instance at most (4,000,000)                         */
+    int32_t fold_every;        /* FP32 sweeps between folds into the FP64 state, even (400)            */
+    int32_t use_graphs;        /* replay the sweeps between folds from a captured CUDA graph (1)       */
+} sf_mixed_options;
+
+/* Solves n independent Stokes problems (each as in solveStokes!, with its own
+ * grid size) to err <= eps by FP64 defect correction around FP32
+ * pseudo-transient sweeps.  Every fold_every sweeps the FP32 correction is
+ * added to the FP64 V and P, dt is recomputed from them (compute_dt) and the
+ * FP64 residual is evaluated -- that is the stopping test and the constant
+ * term of the next sweeps.  The sweeps are the reference's PT iteration
+ * (damping, pseudo-time steps, free-slip BCs) on the correction; its damped
+ * rates carry over across folds, so in exact arithmetic the sequence is the
+ * FP64 iteration itself.  One sweep of every instance still iterating is a
+ * single kernel launch over a shared tile list.  opt may be NULL (defaults
+ * above).  Synchronises the stream.  The results are FP32-accurate
+ * corrections of an FP64 solution, not bit-identical to sf_solve_stokes. */
+int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst, int n, const sf_mixed_options* opt,
+                                void* stream);
+
+/* One problem through the batch path; info (may be NULL) receives the
+ * per-instance results. */
+int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy,
+                          const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s, double g_y,
+                          double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
+                          int use_free_surface_stabilization, double eps, double rel_tol,
+                          const sf_mixed_options* opt, void* stream, sf_batch_instance* info);
+
+/* ---------------------------------------------------------------------- */
 /* RK4 marker advection and rebinning                                        */
 /* ---------------------------------------------------------------------- */
 /* Replaces moveMarkersRK4!(x_m, y_m, Vx, Vy, x_vx_min, y_vx_min, x_vy_min,

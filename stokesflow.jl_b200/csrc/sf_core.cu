@@ -286,7 +286,8 @@ int sf_ctx_create(int device, sf_ctx** out) {
         cudaMalloc(&c->d_flags, sizeof(int) * 4) != cudaSuccess ||
         cudaMallocHost(&c->h_scalars, sizeof(double) * SC_N) != cudaSuccess ||
         cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess ||
-        cudaEventCreate(&c->ev_c) != cudaSuccess || cudaEventCreate(&c->ev_d) != cudaSuccess) {
+        cudaEventCreate(&c->ev_c) != cudaSuccess || cudaEventCreate(&c->ev_d) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->work, cudaStreamNonBlocking) != cudaSuccess) {
         cudaError_t le = cudaGetLastError();
         sf_ctx_destroy(c);
         return cuda_fail(le, "sf_ctx_create allocation", __FILE__, __LINE__);
@@ -303,12 +304,14 @@ int sf_ctx_destroy(sf_ctx* c) {
     if (!c) return SF_OK;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
-    Scratch* all[] = {&c->keys, &c->counts, &c->offsets, &c->cursor, &c->perm, &c->scan_tmp, &c->fields, &c->partials};
+    Scratch* all[] = {&c->keys, &c->counts,   &c->offsets,  &c->cursor, &c->perm,
+                      &c->scan_tmp, &c->fields, &c->partials, &c->mixed};
     for (Scratch* s : all)
         if (s->ptr) cudaFree(s->ptr);
     if (c->d_counters) cudaFree(c->d_counters);
     if (c->d_scalars) cudaFree(c->d_scalars);
     if (c->d_flags) cudaFree(c->d_flags);
+    if (c->work) cudaStreamDestroy(c->work);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     cudaEvent_t evs[] = {c->ev_a, c->ev_b, c->ev_c, c->ev_d};
     for (cudaEvent_t ev : evs)
@@ -319,7 +322,8 @@ int sf_ctx_destroy(sf_ctx* c) {
 
 int sf_ctx_scratch_bytes(sf_ctx* c, int64_t* bytes) {
     if (!c || !bytes) return fail(SF_ERR_INVALID_ARG, "sf_ctx_scratch_bytes: NULL argument");
-    const Scratch* all[] = {&c->keys, &c->counts, &c->offsets, &c->cursor, &c->perm, &c->scan_tmp, &c->fields, &c->partials};
+    const Scratch* all[] = {&c->keys,     &c->counts, &c->offsets,  &c->cursor, &c->perm,
+                            &c->scan_tmp, &c->fields, &c->partials, &c->mixed};
     int64_t b = 0;
     for (const Scratch* s : all) b += (int64_t)s->bytes;
     *bytes = b;

@@ -65,8 +65,9 @@ struct sf_ctx {
     int num_sms = 148;
     // deposit / rebin scratch
     sf::Scratch keys, counts, offsets, cursor, perm, scan_tmp;
-    // PT solve: padded internal fields, reduction partials
-    sf::Scratch fields, partials;
+    // PT solve: padded internal fields, reduction partials; mixed/batched engine arena
+    sf::Scratch fields, partials, mixed;
+    cudaStream_t work = nullptr;  // private non-blocking stream (graph capture needs a non-legacy stream)
     // device counters (unsigned long long[CNT_N]) and scalars (double[SC_N])
     unsigned long long* d_counters = nullptr;
     double* d_scalars = nullptr;

@@ -534,7 +534,19 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_
                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
+static int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int esize, const void* base, int64_t ld,
+                       int64_t rows, int box_w, int box_h);
+
 int encode_tmap_f64(CUtensorMap* map, const double* base, int64_t ld, int64_t rows, int box_w, int box_h) {
+    return encode_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, base, ld, rows, box_w, box_h);
+}
+
+int encode_tmap_f32(CUtensorMap* map, const float* base, int64_t ld, int64_t rows, int box_w, int box_h) {
+    return encode_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ld, rows, box_w, box_h);
+}
+
+static int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int esize, const void* base, int64_t ld,
+                       int64_t rows, int box_w, int box_h) {
     static PFN_encodeTiled fn = nullptr;
     if (!fn) {
         void* p = nullptr;
@@ -545,10 +557,10 @@ int encode_tmap_f64(CUtensorMap* map, const double* base, int64_t ld, int64_t ro
         fn = (PFN_encodeTiled)p;
     }
     cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)ld * 8};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * (cuuint64_t)esize};
     cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, (void*)base, dims, strides, box, estr,
+    CUresult r = fn(map, dtype, 2, (void*)base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(SF_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");

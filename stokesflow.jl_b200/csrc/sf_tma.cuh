@@ -71,5 +71,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 // host: encode a 2-D FP64 tensor map over a (rows x ld) row-major buffer
 // (inner dimension ld elements, row pitch ld*8 bytes), box = box_w x box_h.
 int encode_tmap_f64(CUtensorMap* map, const double* base, int64_t ld, int64_t rows, int box_w, int box_h);
+int encode_tmap_f32(CUtensorMap* map, const float* base, int64_t ld, int64_t rows, int box_w, int box_h);
 
 }  // namespace sf

@@ -51,6 +51,26 @@ class Warnings(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchInstance(C.Structure):
+    """sf_batch_instance."""
+    _fields_ = [("P", _vp), ("Vx_pad", _vp), ("Vy_pad", _vp), ("rho_vy", _vp), ("mu_b", _vp), ("mu_p", _vp),
+                ("Vx_s", _vp), ("Vy_s", _vp), ("Nx", _i64), ("Ny", _i64), ("g_y", _d), ("dx", _d), ("dy", _d),
+                ("dt", _d), ("maxdisp", _d), ("eps", _d), ("rel_tol", _d),
+                ("use_free_surface_stabilization", _i32), ("reserved0", _i32), ("dt_out", _d), ("err", _d),
+                ("eps_used", _d), ("inner_iters", _i64), ("outer_iters", _i64), ("converged", _i32),
+                ("status", _i32), ("batch_ms", _d)]
+
+    RESULTS = ("dt_out", "err", "eps_used", "inner_iters", "outer_iters", "converged", "status", "batch_ms")
+
+    def results(self):
+        return {k: getattr(self, k) for k in self.RESULTS}
+
+
+class MixedOptions(C.Structure):
+    """sf_mixed_options."""
+    _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32)]
+
+
 class PlumeModelC(C.Structure):
     """sf_plume_model."""
     _fields_ = [(n, _d) for n in ("air_height", "plume_x", "plume_y", "plume_r", "rho_air", "rho_matrix",
@@ -73,6 +93,9 @@ PROTOTYPES = {
     "sf_solve_stokes": (C.c_int, [_vp] + [_pd] * 19 + [_d, _d, _d, _i64, _i64, _d, _d, C.c_int, _d, C.c_int, _i64,
                                                        _vp, C.POINTER(SolveInfo)]),
     "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),
+    "sf_solve_stokes_batch_mixed": (C.c_int, [_vp, C.POINTER(BatchInstance), C.c_int, C.POINTER(MixedOptions), _vp]),
+    "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64, _d, _d,
+                                        C.c_int, _d, _d, C.POINTER(MixedOptions), _vp, C.POINTER(BatchInstance)]),
     "sf_move_markers_rk4": (C.c_int, [_vp, _pd, _pd, _i64, _pd, _i64, _i64, _pd, _i64, _i64, _d, _d, _d, _d, _d, _d,
                                       _d, _d, _d, _vp]),
     "sf_rebin_markers": (C.c_int, [_vp, _pd, _pd, _i64, _d, _d, _d, _d, _i64, _i64, _pd, _pd, _pd, _vp]),

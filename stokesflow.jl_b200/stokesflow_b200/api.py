@@ -205,6 +205,51 @@ def solve_stokes(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtP
     return r["dt"], r["T_eff"], r["runtime"]
 
 
+class MixedProblem:
+    """One Stokes problem for the mixed-precision / batched solver: the caller arrays of
+    :func:`solve_stokes` (state in/out) and its scalars.  ``eps`` is absolute; ``rel_tol`` > 0
+    replaces it by rel_tol * mean|g_y rho_vy|.  After a solve, ``result`` holds dt_out, err,
+    inner/outer iteration counts and the convergence flag."""
+
+    def __init__(self, P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp,
+                 eps=1e-8, rel_tol=0.0, use_free_surface_stabilization=True):
+        Nx, Ny = int(Nx), int(Ny)
+        self.arrays = dict(P=P, Vx_pad=Vx_pad, Vy_pad=Vy_pad, rho_vy=rho_vy, mu_b=mu_b, mu_p=mu_p, Vx_s=Vx_s,
+                           Vy_s=Vy_s)
+        shapes = dict(P=(Nx - 1, Ny - 1), Vx_pad=(Nx + 2, Ny + 1), Vy_pad=(Nx + 1, Ny + 2), rho_vy=(Nx + 1, Ny),
+                      mu_b=(Nx, Ny), mu_p=(Nx - 1, Ny - 1), Vx_s=(Nx, Ny + 1), Vy_s=(Nx + 1, Ny))
+        c = _lib.BatchInstance()
+        for k, a in self.arrays.items():
+            setattr(c, k, _grid(a, k, shapes[k]))
+        c.Nx, c.Ny = Nx, Ny
+        c.g_y, c.dx, c.dy, c.dt, c.maxdisp = float(g_y), float(dx), float(dy), float(dt), float(maxdisp)
+        c.eps, c.rel_tol = float(eps), float(rel_tol)
+        c.use_free_surface_stabilization = int(bool(use_free_surface_stabilization))
+        self.c = c
+        self.result = None
+
+
+def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True):
+    """Options of the mixed-precision / batched solver (sf_mixed_options)."""
+    return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)))
+
+
+def solve_stokes_batch_mixed(problems, *, options=None, ctx: Context | None = None, stream=None):
+    """Solve a list of :class:`MixedProblem` (independent, any grid sizes) with FP64 defect correction
+    around FP32 PT sweeps, all instances sharing each sweep launch.  Returns the per-instance results."""
+    arr = (_lib.BatchInstance * len(problems))(*[p.c for p in problems])
+    opt = options if options is not None else mixed_options()
+    c = _ctx(ctx)
+    check(lib().sf_solve_stokes_batch_mixed(c.handle, arr, len(problems), C.byref(opt), _stream(stream)),
+          "solve_stokes_batch_mixed")
+    out = []
+    for p, r in zip(problems, arr):
+        p.c = r
+        p.result = r.results()
+        out.append(p.result)
+    return out
+
+
 def residual_scale(rho_vy, Nx, Ny, g_y, *, ctx: Context | None = None, stream=None) -> float:
     """mean |g_y rho_vy| over the Ry interior: eps = rtol * residual_scale(...) is a relative stopping test."""
     out = C.c_double()

@@ -21,6 +21,11 @@ import torch
 from . import api
 
 
+# HBM bytes of one FP32 sweep per point: read dVx, dVy, dP, mu_b, mu_p, rho, rdiv, the two damped rates and
+# the two momentum residuals, write dVx, dVy, dP and the two rates (11 reads + 5 writes of 4 bytes)
+MIXED_BYTES_PER_POINT = 64
+
+
 def node_origins(dx, dy):
     """First coordinates of the staggered node sets (StokesFlow2D_multixpu.jl:117-126)."""
     return dict(x=0.0, y=0.0, x_p=0.0 * dx + 0.5 * dx, y_p=0.0 * dy + 0.5 * dy, x_vx=(1 - 2) * dx,
@@ -61,6 +66,9 @@ class StokesFlow2D:
     device: str = "cuda"
     keep_work_arrays: bool = True     # allocate tau, divV, dtau, R like the reference
     host_markers: bool = False        # markers start in pinned host memory (end-to-end path)
+    solver: str = "fp64"              # "fp64": plain path, bit-identical to the reference; "mixed": FP32 sweeps +
+                                      # FP64 defect correction
+    mixed_opts: object = None
     ctx: api.Context | None = None
     history: list = field(default_factory=list)
 
@@ -135,7 +143,19 @@ class StokesFlow2D:
             return self.stokes_eps
         return self.stokes_rtol * api.residual_scale(self.rho_vy, self.Nx, self.Ny, self.g_y, ctx=self.ctx)
 
+    def mixed_problem(self):
+        """This timestep's Stokes problem for the mixed-precision / batched solver."""
+        return api.MixedProblem(self.P, self.Vx, self.Vy, self.rho_vy, self.mu_b, self.mu_p, self.Vx_s, self.Vy_s,
+                                self.g_y, self.dx, self.dy, self.Nx, self.Ny, self.dt, self.maxdisp,
+                                eps=self.stokes_eps, rel_tol=self.stokes_rtol or 0.0)
+
     def solve(self):
+        if self.solver == "mixed":
+            p = self.mixed_problem()
+            r = api.solve_stokes_batch_mixed([p], options=self.mixed_opts, ctx=self.ctx)[0]
+            self.dt = r["dt_out"]
+            return dict(r, dt=r["dt_out"], iters=r["inner_iters"], loop_ms=r["batch_ms"],
+                        bytes_per_iter=float(MIXED_BYTES_PER_POINT * (self.Nx - 1) * (self.Ny - 1)))
         info = api.solve_stokes_info(self.P, self.Vx, self.Vy, self.rho_vy, self.mu_b, self.mu_p, self.txx, self.tyy,
                                      self.txy, self.divV, self.dtPt, self.Rx, self.Ry, self.dVxdt, self.dVydt,
                                      self.dtVx, self.dtVy, self.Vx_s, self.Vy_s, self.g_y, self.dx, self.dy, self.Nx,
