@@ -67,7 +67,28 @@ def parse():
     ap.add_argument("--pt-probe", type=int, default=0, metavar="ITERS",
                     help="kernel probe: run ITERS fused PT iterations of an n x n solve (smooth random fields, no "
                          "markers) and print the kernel time; used for ncu captures")
+    ap.add_argument("--form", default="timestep", choices=["timestep", "batch", "serve"],
+                    help="timestep: the plain FP64 timestep (default line); batch: many independent solves in one "
+                         "engine vs a loop of plain FP64 solves; serve: a Poisson request stream, continuous "
+                         "batching vs plain FP64 serving")
+    ap.add_argument("--batch-instances", type=int, default=256)
+    ap.add_argument("--batch-cells", default="127,1023", help="cells per side, log-uniform range")
+    ap.add_argument("--mu-log10", default="-2,1", help="inclusion viscosity range (log10), log-uniform")
+    ap.add_argument("--fp64-sample", type=int, default=0,
+                    help="batch form: time the FP64 loop on the first K instances only (0: all)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="requests per second (Poisson)")
+    ap.add_argument("--serve-cells", default="63,511", help="cells per side of a request, log-uniform range")
+    ap.add_argument("--serve-steps", default="1,20", help="timesteps per request, uniform range")
+    ap.add_argument("--hbm-budget-gb", type=float, default=64.0)
+    ap.add_argument("--fold-every", type=int, default=400)
     return ap.parse_args()
+
+
+def _pair(s, typ=float):
+    a, b = s.split(",")
+    return typ(a), typ(b)
 
 
 def pt_probe(a):
@@ -322,6 +343,161 @@ def _cpu_model():
     return None
 
 
+# ---------------------------------------------------------------------------
+# batched and served forms (single GPU; printed as their own JSON lines)
+# ---------------------------------------------------------------------------
+SOLVE_CAP = 4_000_000   # PT iterations / FP32 sweeps a solve may take in the batch and serve forms
+
+
+def _deposit_instances(sf, specs):
+    """rho_vy, mu_b, mu_p of every instance deposited from its markers (markers freed afterwards)."""
+    out = []
+    for sp in specs:
+        st = sf.StokesFlow2D(sp.Nx, sp.Ny, 1.0, 1.0, sp.model, marker_density=sp.md, jitter=0.5, seed=sp.seed,
+                             keep_work_arrays=False)
+        st.deposit()
+        out.append(dict(spec=sp, rho_vy=st.rho_vy, mu_b=st.mu_b, mu_p=st.mu_p, dx=st.dx, dy=st.dy,
+                        markers=st.n_markers))
+        del st
+    torch.cuda.synchronize()
+    return out
+
+
+def _state_arrays(sf, Nx, Ny):
+    z = sf.zeros
+    return dict(P=z(Nx - 1, Ny - 1), Vx_pad=z(Nx + 2, Ny + 1), Vy_pad=z(Nx + 1, Ny + 2), Vx_s=z(Nx, Ny + 1),
+                Vy_s=z(Nx + 1, Ny), dVx=z(Nx - 2, Ny - 1), dVy=z(Nx - 1, Ny - 2))
+
+
+def _rel_l2(a, b):
+    d = torch.linalg.vector_norm((a - b).flatten()).item()
+    n = torch.linalg.vector_norm(b.flatten()).item()
+    return d / n if n > 0 else d
+
+
+def run_batch_form(a):
+    """Batching form: N independent problems (seeded random grids and inclusion layouts) solved to relative
+    residual rtol in ONE engine run (FP32 sweeps + FP64 defect correction, one launch per sweep for all
+    instances, graph replay) against a loop of plain FP64 solves of the same problems."""
+    import stokesflow_b200 as sf
+    from stokesflow_b200 import workloads
+    torch.cuda.set_device(0)
+    specs = workloads.batch_specs(a.batch_instances, a.seed, cells=_pair(a.batch_cells, int),
+                                  mu_log10=_pair(a.mu_log10), mu_air=a.mu_air)
+    inst = _deposit_instances(sf, specs)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+
+    def mixed_problems(subset):
+        probs, arrs = [], []
+        for d in subset:
+            sp = d["spec"]
+            s = _state_arrays(sf, sp.Nx, sp.Ny)
+            arrs.append(s)
+            probs.append(sf.MixedProblem(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"],
+                                         s["Vx_s"], s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5,
+                                         rel_tol=a.rtol))
+        return probs, arrs
+
+    def fp64_solve(d, s):
+        sp = d["spec"]
+        scale = sf.residual_scale(d["rho_vy"], sp.Nx, sp.Ny, 9.81)
+        return sf.solve_stokes_info(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"], None, None,
+                                    None, None, None, None, None, s["dVx"], s["dVy"], None, None, s["Vx_s"],
+                                    s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5, eps=a.rtol * scale,
+                                    iter_max=SOLVE_CAP)
+
+    # warm-up of both paths on the two smallest instances (graph capture, occupancy queries, scratch growth)
+    small = sorted(inst, key=lambda d: d["spec"].points)[:2]
+    sf.solve_stokes_batch_mixed(mixed_problems(small)[0], options=opts)
+    for d in small:
+        fp64_solve(d, _state_arrays(sf, d["spec"].Nx, d["spec"].Ny))
+    probs, arrs = mixed_problems(inst)
+    k = a.fp64_sample if a.fp64_sample > 0 else len(inst)
+    fp64_arrs = [_state_arrays(sf, d["spec"].Nx, d["spec"].Ny) for d in inst[:k]]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(0)
+    clocks.start()
+    e0.record()
+    res = sf.solve_stokes_batch_mixed(probs, options=opts)
+    e1.record()
+    torch.cuda.synchronize()
+    mixed_s = e0.elapsed_time(e1) / 1e3
+    e0.record()
+    infos = [fp64_solve(d, s) for d, s in zip(inst[:k], fp64_arrs)]
+    e1.record()
+    torch.cuda.synchronize()
+    fp64_s = e0.elapsed_time(e1) / 1e3
+    clk = clocks.stop()
+    errs = {f: sorted(_rel_l2(arrs[q][f], fp64_arrs[q][f]) for q in range(k)
+                      if res[q]["status"] == 0 and infos[q]["converged"]) for f in ("Vx_pad", "Vy_pad", "P")}
+    pts = [d["spec"].points for d in inst]
+    mixed_rate = len(inst) / mixed_s
+    fp64_rate = k / fp64_s
+    mixed_sweeps = sum(r["inner_iters"] for r in res)
+    return {"form": "batch", "metric": f"Stokes solves/s to relative residual {a.rtol:g}, independent instances",
+            "unit": "solves/s", "value": round(mixed_rate, 3), "fp64_loop_value": round(fp64_rate, 3),
+            "speedup_vs_fp64_loop": round(mixed_rate / fp64_rate, 3), "higher_is_better": True,
+            "mixed_s": round(mixed_s, 3), "fp64_s": round(fp64_s, 3), "fp64_instances_timed": k,
+            "instances": len(inst), "converged": sum(r["converged"] for r in res),
+            "nonfinite": sum(1 for r in res if r["status"] == 5),
+            "fp64_converged": sum(int(i["converged"]) for i in infos),
+            "mixed_sweeps_total": int(mixed_sweeps), "fp64_iters_total": int(sum(i["iters"] for i in infos)),
+            "fp32_sweep_gpts": round(sum(r["inner_iters"] * pts[q] for q, r in enumerate(res)) / mixed_s / 1e9, 3),
+            "rel_l2_vs_fp64": {f: {"median": v[len(v) // 2] if v else None, "max": v[-1] if v else None}
+                               for f, v in errs.items()},
+            "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
+            "clocks": clk,
+            "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {a.batch_cells}, 9-25 "
+                                   f"markers/cell, 1-3 inclusions mu log10-uniform {a.mu_log10}, air mu "
+                                   f"{a.mu_air:g}", "grid_points_total": int(sum(pts)),
+                       "markers_total": int(sum(d['markers'] for d in inst)), "fold_every": a.fold_every,
+                       "seed": a.seed, "solve_cap": SOLVE_CAP}}
+
+
+def run_serve_form(a):
+    """Serving form: a Poisson stream of StokesFlow2D requests (1-20 timesteps each, random grids and
+    inclusion layouts), continuous batching through the resident engine against plain FP64 serving (one
+    request at a time, arrival order), on the same request trace."""
+    import stokesflow_b200 as sf
+    from stokesflow_b200 import serving
+    torch.cuda.set_device(0)
+    kw = dict(cells=_pair(a.serve_cells, int), timesteps=_pair(a.serve_steps, int), mu_log10=_pair(a.mu_log10),
+              mu_air=a.mu_air)
+    budget = int(a.hbm_budget_gb * 2 ** 30)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+    # warm-up: one small request through each server
+    for solver in ("mixed", "fp64"):
+        w = serving.poisson_requests(1, 0.0, a.seed + 1, cells=(31, 31), timesteps=(1, 1))
+        srv = serving.StokesServer(budget // 8, solver=solver, rtol=a.rtol, options=opts, iter_max=SOLVE_CAP)
+        srv.run(w)
+        srv.close()
+    clocks = ClockSampler(0)
+    clocks.start()
+    out = {}
+    for solver in ("mixed", "fp64"):
+        reqs = serving.poisson_requests(a.serve_requests, a.serve_rate, a.seed, **kw)
+        srv = serving.StokesServer(budget, solver=solver, rtol=a.rtol, options=opts, iter_max=SOLVE_CAP)
+        out[solver] = srv.run(reqs)
+        out[solver]["peak_state_bytes"] = srv.peak_state
+        if srv.engine is not None:
+            out[solver]["engine"] = srv.engine.stats()
+        srv.close()
+    clk = clocks.stop()
+    m, f = out["mixed"], out["fp64"]
+    return {"form": "serve", "metric": f"p50/p99 request latency and solves/s at relative residual {a.rtol:g}",
+            "unit": "s / solves/s", "p50_latency_s": round(m["p50_latency_s"], 4),
+            "p99_latency_s": round(m["p99_latency_s"], 4), "solves_per_s": round(m["solves_per_s"], 3),
+            "fp64_p50_latency_s": round(f["p50_latency_s"], 4), "fp64_p99_latency_s": round(f["p99_latency_s"], 4),
+            "fp64_solves_per_s": round(f["solves_per_s"], 3),
+            "speedup_solves_per_s": round(m["solves_per_s"] / f["solves_per_s"], 3),
+            "mixed": m, "fp64": f, "clocks": clk, "data": "synthetic (seeded Poisson trace, random inclusion layouts)",
+            "config": {"workload": f"{a.serve_requests} requests at {a.serve_rate:g}/s, square grids with cells per "
+                                   f"side log-uniform {a.serve_cells}, {a.serve_steps} timesteps, 9-25 markers/cell, "
+                                   f"inclusion mu log10-uniform {a.mu_log10}",
+                       "hbm_budget_bytes": budget, "fold_every": a.fold_every, "seed": a.seed}}
+
+
 def run_reference(a, rank):
     if rank != 0:
         return None
@@ -358,6 +534,11 @@ def main():
     if a.pt_probe:
         torch.cuda.set_device(local_rank)
         pt_probe(a)
+        return
+    if a.form != "timestep" and a.impl == "ours":
+        if rank == 0:
+            out = run_batch_form(a) if a.form == "batch" else run_serve_form(a)
+            print(json.dumps(out), flush=True)
         return
     if a.impl == "reference":
         out = run_reference(a, rank)

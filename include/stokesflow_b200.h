@@ -39,7 +39,9 @@ typedef enum {
     SF_ERR_OOM = 3,           /* scratch allocation failed                                              */
     SF_ERR_NO_DEVICE = 4,     /* no CUDA device / device index out of range                             */
     SF_ERR_NONFINITE = 5,     /* the PT iteration produced NaN/Inf (err is not finite)                  */
-    SF_ERR_TOO_LARGE = 6      /* a size exceeds what the entry point supports                           */
+    SF_ERR_TOO_LARGE = 6,     /* a size exceeds what the entry point supports                           */
+    SF_ERR_BUSY = 7           /* an engine's arena or instance table is full now; retry once instances
+                                 have finished (admission control, sf_engine_submit)                    */
 } sf_status;
 
 typedef struct sf_ctx sf_ctx;
@@ -192,13 +194,21 @@ typedef struct {
     int64_t outer_iters;       /* FP64 residual evaluations          */
     int32_t converged;
     int32_t status;            /* sf_status of this instance         */
-    double batch_ms;           /* device time of the whole batch     */
+    double batch_ms;           /* sf_solve_stokes_batch_mixed: device time of the whole batch;
+                                  sf_engine: host time from submit to the step that finished it */
 } sf_batch_instance;
 
 typedef struct {
     int64_t max_sweeps;        /* FP32 sweeps per instance at most (4,000,000)                         */
     int32_t fold_every;        /* FP32 sweeps between folds into the FP64 state, even (400)            */
     int32_t use_graphs;        /* replay the sweeps between folds from a captured CUDA graph (1)       */
+    int32_t dtau_local_max;    /* 1: pseudo-time step of a velocity node from the largest viscosity of
+                                  its stencil (both pressure cells, both shear nodes), which converges
+                                  faster on soft inclusions; 0: the reference's average
+                                  (StokesSolver_multixpu.jl:129-130).  The converged solution is the
+                                  same either way.  Neither form converges on inclusions much stiffer
+                                  than their matrix (100x diverges in FP64 too) (0)                   */
+    int32_t reserved;
 } sf_mixed_options;
 
 /* Solves n independent Stokes problems (each as in solveStokes!, with its own
@@ -223,6 +233,61 @@ int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad
                           double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
                           int use_free_surface_stabilization, double eps, double rel_tol,
                           const sf_mixed_options* opt, void* stream, sf_batch_instance* info);
+
+/* ---------------------------------------------------------------------- */
+/* resident solve engine: continuous batching for a serving loop           */
+/* ---------------------------------------------------------------------- */
+/* The engine behind sf_solve_stokes_batch_mixed, kept alive between calls so
+ * that instances can join and leave while others iterate.  It owns a device
+ * arena of arena_bytes (the HBM budget of its solves) and a table of at most
+ * max_instances instances.  Each sf_engine_step is one round: every admitted
+ * instance folds its correction, gets its FP64 residual and stopping test;
+ * the finished ones are written back to their caller arrays and leave (arena
+ * space and table slot free at once); the rest run fold_every FP32 sweeps
+ * (one launch per sweep over all of them, graph-replayed).  An instance's
+ * arithmetic and stopping decisions depend on itself alone, so its results
+ * are bit-identical whatever else is in the engine and whenever it joined. */
+typedef struct sf_engine sf_engine;
+
+typedef struct {
+    int64_t arena_bytes;       /* budget                                        */
+    int64_t arena_used;        /* bytes held by admitted instances              */
+    int64_t arena_peak;
+    int64_t submitted, finished, rounds;
+    int64_t sweeps;            /* FP32 sweep launches (one covers all instances) */
+    int32_t active;            /* admitted, not finished                         */
+    int32_t pending_results;   /* finished, not yet reported by sf_engine_step   */
+} sf_engine_stats;
+
+/* Arena bytes one instance of Nx x Ny grid points holds while admitted. */
+int sf_engine_instance_bytes(int64_t Nx, int64_t Ny, int64_t* bytes);
+
+/* opt may be NULL (the defaults of sf_mixed_options).  The arena is
+ * allocated here, once. */
+int sf_engine_create(sf_ctx* ctx, int64_t arena_bytes, int32_t max_instances, const sf_mixed_options* opt,
+                     sf_engine** out);
+/* Waits for the engine's work, then frees it.  Instances still admitted are
+ * dropped (their caller arrays keep what they held). */
+int sf_engine_destroy(sf_engine* e);
+
+/* Admits one instance: its inputs are read after the work already queued on
+ * `stream` (a stream dependency, no host wait).  *inst must stay valid until
+ * sf_engine_step reports its ticket; the results are then in its arrays and
+ * fields.  SF_ERR_BUSY: no room in the arena or the table right now (nothing
+ * admitted); SF_ERR_TOO_LARGE: the instance can never fit this arena. */
+int sf_engine_submit(sf_engine* e, sf_batch_instance* inst, void* stream, int64_t* ticket);
+
+/* One round (see above).  Up to `cap` tickets of finished instances go to
+ * finished[] (*n_finished of them; more stay pending for the next call);
+ * `stream` is made to wait for their write-back, so work queued on it after
+ * this call sees their results.  Returns once the round's sweeps are queued
+ * (they run while the host goes on).  *n_active: instances still admitted
+ * (either output pointer may be NULL).  After an error status other than
+ * SF_ERR_BUSY, destroy the engine. */
+int sf_engine_step(sf_engine* e, void* stream, int64_t* finished, int32_t cap, int32_t* n_finished,
+                   int32_t* n_active);
+
+int sf_engine_get_stats(sf_engine* e, sf_engine_stats* stats);
 
 /* ---------------------------------------------------------------------- */
 /* RK4 marker advection and rebinning                                        */

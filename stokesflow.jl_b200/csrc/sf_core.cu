@@ -259,6 +259,7 @@ const char* sf_status_string(int status) {
         case SF_ERR_NO_DEVICE: return "no CUDA device";
         case SF_ERR_NONFINITE: return "non-finite residual";
         case SF_ERR_TOO_LARGE: return "size exceeds the supported maximum";
+        case SF_ERR_BUSY: return "engine full; retry after instances finish";
         default: return "unknown status";
     }
 }
@@ -304,6 +305,7 @@ int sf_ctx_destroy(sf_ctx* c) {
     if (!c) return SF_OK;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
+    mixed_engine_release(c);
     Scratch* all[] = {&c->keys, &c->counts,   &c->offsets,  &c->cursor, &c->perm,
                       &c->scan_tmp, &c->fields, &c->partials, &c->mixed};
     for (Scratch* s : all)

@@ -75,6 +75,7 @@ struct sf_ctx {
     int* d_flags = nullptr;       // device error flags (int[4]); [0]: a bounded wait timed out
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
     int64_t launches = 0;         // kernels launched through this context
+    sf_engine* batch_engine = nullptr;  // the engine sf_solve_stokes_batch_mixed reuses across calls
 };
 
 namespace sf {
@@ -82,6 +83,8 @@ namespace sf {
 // Ensures `s` holds at least `bytes`; contents are not preserved.
 int ensure(sf_ctx* ctx, Scratch& s, size_t bytes);
 int set_device(sf_ctx* ctx);
+// frees the context's cached batch engine (sf_mixed.cu)
+void mixed_engine_release(sf_ctx* ctx);
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

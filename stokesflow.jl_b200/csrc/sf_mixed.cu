@@ -29,9 +29,14 @@
 // The FP32 sweeps are not bit-compatible with the plain FP64 path (nothing can
 // be at FP32); their accuracy is measured against the FP64 oracle.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <iterator>
+#include <map>
+#include <string>
 #include <type_traits>
 #include <vector>
 
@@ -74,7 +79,7 @@ struct Inst {  // device-side description of one instance
     int parity;             // which dV/dP buffer is "in" at launch parity 0
     double dx, dy, _dx, _dy, g_y, dt, dt_cfl, dt_in, maxdisp;
     int use_stab;
-    int pad_;
+    int dtau_max;           // pseudo-time step from the stencil's largest viscosity
 };
 
 __device__ __forceinline__ float* gf(const Inst& I, int k) { return I.f32 + (int64_t)k * I.fstride32; }
@@ -209,7 +214,11 @@ __global__ void __launch_bounds__(NT, 3) k_pt32(const CUtensorMap* __restrict__ 
                            (sPn[b][a + 1] - sPn[b][a]) * _dx + sRx[b][a];
                 float dv = I.dampXf * sRvx[b][a] + Rx;
                 Rvx[o] = dv;
-                float dtau = I.c_vscf / ((sMup[b][a] + sMup[b][a + 1]) * 0.5f);
+                // pseudo-time step: the reference's average of the two pressure-cell viscosities
+                // (:129), or the largest viscosity of the node's stencil (stable at high contrast)
+                float mux = I.dtau_max ? fmaxf(fmaxf(sMup[b][a], sMup[b][a + 1]), fmaxf(sMub[b][a + 1], sMub[b + 1][a + 1]))
+                                       : (sMup[b][a] + sMup[b][a + 1]) * 0.5f;
+                float dtau = I.c_vscf / mux;
                 float vn = sVx[b + 1][a + 1] + dtau * dv;
                 Vx_out[o + 1 + LD] = vn;
                 if (j == 0) Vx_out[o + 1] = vn;
@@ -224,7 +233,9 @@ __global__ void __launch_bounds__(NT, 3) k_pt32(const CUtensorMap* __restrict__ 
                            I.g_dtf * (av * dxr * 0.5f * _dx + sVy[b + 1][a + 1] * dyr * 0.5f * _dy) + sRy[b][a];
                 float dv = I.dampYf * sRvy[b][a] + Ry;
                 Rvy[o] = dv;
-                float dtau = I.c_vscf / ((sMup[b][a] + sMup[b + 1][a]) * 0.5f);
+                float muy = I.dtau_max ? fmaxf(fmaxf(sMup[b][a], sMup[b + 1][a]), fmaxf(sMub[b + 1][a], sMub[b + 1][a + 1]))
+                                       : (sMup[b][a] + sMup[b + 1][a]) * 0.5f;
+                float dtau = I.c_vscf / muy;
                 float vn = sVy[b + 1][a + 1] + dtau * dv;
                 Vy_out[o + 1 + LD] = vn;
                 if (i == 0) Vy_out[o + LD] = vn;
@@ -404,8 +415,9 @@ __global__ void k_inst_dt(Inst* __restrict__ insts, const Seg* __restrict__ segs
     }
 }
 
+// per instance of the round: {err, residual scale, dt_cfl} -> out[3 q ..]
 __global__ void k_inst_err(const Seg* __restrict__ segs, const double* __restrict__ part, const Inst* __restrict__ insts,
-                           double* __restrict__ err_out) {
+                           const double* __restrict__ scale, double* __restrict__ out) {
     __shared__ double sh[32];
     const Seg g = segs[blockIdx.x];
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -424,7 +436,9 @@ __global__ void k_inst_err(const Seg* __restrict__ segs, const double* __restric
         if (bb > m || bb != bb) m = bb;
         if (cc > m || cc != cc) m = cc;
         if (a != a) m = a;
-        err_out[blockIdx.x] = m;
+        out[3 * blockIdx.x] = m;
+        out[3 * blockIdx.x + 1] = scale[g.inst];
+        out[3 * blockIdx.x + 2] = I.dt_cfl;
     }
 }
 
@@ -506,75 +520,98 @@ __global__ void k_rho_scale64(const double* __restrict__ rho, int Nx, int Ny, do
 }  // namespace sf
 
 // ===========================================================================
-// host side: the batch engine
+// host side: the resident engine
 // ===========================================================================
 namespace sf {
 namespace mx {
 
-enum Phase { PH_OUTER = 0, PH_INNER = 1, PH_DONE = 2 };
-
-struct HostInst {
-    sf_batch_instance* user;
-    Inst d;                  // device copy source
-    int64_t tile0, ntiles;   // tiles of this instance in the full tile list
-    int phase = PH_OUTER;
-    int cur = 0;             // physical buffer (0 = A, 1 = B) holding the current correction
-    int64_t inner_here = 0;  // FP32 sweeps in the current correction
-    int64_t inner_total = 0;
-    int64_t outer = 0;
-    double err = 0.0, target = 0.0, eps = 0.0;
-    bool accumulated = true; // nothing to add before the first residual
-};
-
-struct Engine {
-    sf_ctx* ctx;
-    cudaStream_t s;
-    sf_mixed_options opt;
-    std::vector<HostInst> in;
-    // device
-    Inst* d_insts = nullptr;
-    CUtensorMap* d_maps = nullptr;
-    int2* d_tiles = nullptr;
-    int* d_ntiles = nullptr;
-    double* d_part64 = nullptr;
-    Seg* d_segs = nullptr;
-    double* d_err = nullptr;
-    int* d_list = nullptr;
-    double* d_scale = nullptr;
-    // host scratch (pinned)
-    double* h_err = nullptr;
-    int64_t total_tiles = 0;
-    int h_ntiles = 0;         // host copy of the sweep tile count (source of an async upload)
-    int64_t launches = 0;     // k_pt32 launches so far (their parity alternates)
-    int pt_blocks = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    int graph_k = 0;
-
-    ~Engine() {
-        if (gexec) cudaGraphExecDestroy(gexec);
-        if (graph) cudaGraphDestroy(graph);
-    }
-
-    int upload_inst(int b) {
-        SF_CUDA(cudaMemcpyAsync(d_insts + b, &in[b].d, sizeof(Inst), cudaMemcpyHostToDevice, s));
-        return SF_OK;
-    }
-
-    // tile list + segments of the instances in `ids`; returns the number of tiles
-    int build_lists(const std::vector<int>& ids, int2* h_tiles, Seg* h_segs, int64_t* ntiles_out) {
-        int64_t nt = 0;
-        for (size_t q = 0; q < ids.size(); ++q) {
-            const HostInst& h = in[ids[q]];
-            h_segs[q] = Seg{ids[q], (int)nt, (int)(nt + h.ntiles), 0};
-            for (int64_t k = 0; k < h.ntiles; ++k) h_tiles[nt++] = make_int2(ids[q], (int)k);
-        }
-        *ntiles_out = nt;
-        return SF_OK;
-    }
-};
-
 static unsigned grid1(int64_t n, int per) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, 65535)); }
+
+// arena bytes of one instance: FP32 fields, then FP64 fields, each 256-byte aligned
+struct Layout {
+    int64_t LD, rows, fstride, bytes32, bytes64;
+    Layout(int64_t Nx, int64_t Ny) {
+        LD = round_up(Nx + 4, 32);
+        rows = Ny + 3;
+        fstride = LD * rows;
+        bytes32 = round_up((int64_t)G_NUM * fstride * 4, 256);
+        bytes64 = round_up((int64_t)D_NUM * fstride * 8, 256);
+    }
+    int64_t bytes() const { return bytes32 + bytes64; }
+};
+
+// first-fit allocator over [0, cap) (offsets and sizes multiples of 256), coalescing on release
+class ArenaAlloc {
+   public:
+    void reset(int64_t cap) {
+        free_.clear();
+        if (cap > 0) free_[0] = cap;
+        cap_ = cap;
+        used_ = 0;
+    }
+    int64_t alloc(int64_t bytes) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            const int64_t off = it->first, rest = it->second - bytes;
+            free_.erase(it);
+            if (rest > 0) free_[off + bytes] = rest;
+            used_ += bytes;
+            peak_ = std::max(peak_, used_);
+            return off;
+        }
+        return -1;
+    }
+    void release(int64_t off, int64_t bytes) {
+        used_ -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    int64_t cap() const { return cap_; }
+    int64_t used() const { return used_; }
+    int64_t peak() const { return peak_; }
+
+   private:
+    std::map<int64_t, int64_t> free_;
+    int64_t cap_ = 0, used_ = 0, peak_ = 0;
+};
+
+struct Slot {  // an admitted instance
+    sf_batch_instance* user = nullptr;
+    int64_t ticket = -1;
+    Inst d;                    // source of the device record
+    int64_t ntiles = 0, off = 0, bytes = 0;
+    bool active = false;
+    bool swept = false;        // ran sweeps since its last fold
+    int64_t inner_total = 0, outer = 0;
+    double err = 0.0, eps = 0.0;
+    std::chrono::steady_clock::time_point t_submit;
+};
+
+static sf_mixed_options normalized(const sf_mixed_options* o) {
+    sf_mixed_options r{};
+    if (o) {
+        r = *o;
+    } else {
+        r.max_sweeps = 4000000;
+        r.fold_every = 400;
+        r.use_graphs = 1;
+        r.dtau_local_max = 0;
+    }
+    if (r.fold_every < 2) r.fold_every = 2;
+    r.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
+    return r;
+}
 
 }  // namespace mx
 }  // namespace sf
@@ -582,283 +619,548 @@ static unsigned grid1(int64_t n, int per) { return (unsigned)std::max<int64_t>(1
 using namespace sf;
 using namespace sf::mx;
 
-extern "C" int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst, int n, const sf_mixed_options* o,
-                                           void* stream) {
-    SF_REQUIRE(ctx && inst && n >= 1, "sf_solve_stokes_batch_mixed: bad arguments");
-    int rc = set_device(ctx);
-    if (rc) return rc;
-    Engine E;
-    E.ctx = ctx;
-    // the caller's inputs are ready once its stream is; the engine then works on the context's own
-    // non-blocking stream, where graph capture is allowed, and synchronises it before returning
-    SF_CUDA(cudaStreamSynchronize(as_stream(stream)));
-    E.s = ctx->work;
-    cudaStream_t s = E.s;
-    E.opt = o ? *o : sf_mixed_options{};
-    if (!o) {
-        E.opt.max_sweeps = 4000000;
-        E.opt.fold_every = 400;
-        E.opt.use_graphs = 1;
+struct sf_engine {
+    sf_ctx* ctx = nullptr;
+    sf_mixed_options opt{};
+    cudaStream_t s = nullptr;            // own non-blocking stream (graph capture needs one)
+    unsigned char* arena = nullptr;
+    bool arena_owned = false;
+    ArenaAlloc alloc;
+    std::vector<Slot> slots;
+    std::vector<int> free_slots;
+    // device tables, one allocation: insts | maps | segs | out | scale | list | ntiles | flag
+    void* tables = nullptr;
+    Inst* d_insts = nullptr;
+    CUtensorMap* d_maps = nullptr;
+    Seg* d_segs = nullptr;
+    double* d_out = nullptr;
+    double* d_scale = nullptr;
+    int* d_list = nullptr;
+    int* d_ntiles = nullptr;
+    int* d_flag = nullptr;               // a bounded wait of k_pt32 gave up
+    double* h_out = nullptr;             // pinned mirror of d_out
+    // tile list and per-tile partials, grown on demand
+    int2* d_tiles = nullptr;
+    double* d_part = nullptr;
+    int64_t tile_cap = 0;
+    std::vector<int2> h_tiles;
+    std::vector<Seg> h_segs;
+    int h_ntiles = 0;                    // source of the tile-count upload
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_k = 0;
+    int blocks = 0;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    int64_t next_ticket = 0, submitted = 0, finished = 0, rounds = 0, sweeps = 0;
+    std::deque<int64_t> pending;
+};
+
+namespace {
+
+void drop_graph(sf_engine* e) {
+    if (e->gexec) cudaGraphExecDestroy(e->gexec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->gexec = nullptr;
+    e->graph = nullptr;
+}
+
+void engine_free(sf_engine* e) {
+    if (!e) return;
+    if (e->s) cudaStreamSynchronize(e->s);
+    drop_graph(e);
+    if (e->tables) cudaFree(e->tables);
+    if (e->d_tiles) cudaFree(e->d_tiles);
+    if (e->d_part) cudaFree(e->d_part);
+    if (e->h_out) cudaFreeHost(e->h_out);
+    if (e->arena_owned && e->arena) cudaFree(e->arena);
+    if (e->ev_in) cudaEventDestroy(e->ev_in);
+    if (e->ev_out) cudaEventDestroy(e->ev_out);
+    if (e->s) cudaStreamDestroy(e->s);
+    delete e;
+}
+
+int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options* o) {
+    e->ctx = ctx;
+    e->opt = normalized(o);
+    SF_CUDA(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
+    SF_CUDA(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
+    SF_CUDA(cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming));
+    const size_t n = (size_t)slot_cap;
+    const size_t o_ins = 0, o_map = round_up(o_ins + n * sizeof(Inst), 256);
+    const size_t o_seg = round_up(o_map + n * M_NUM * sizeof(CUtensorMap), 256);
+    const size_t o_out = round_up(o_seg + n * sizeof(Seg), 256);
+    const size_t o_scl = round_up(o_out + n * 3 * 8, 256);
+    const size_t o_lst = round_up(o_scl + n * 8, 256);
+    const size_t o_nt = round_up(o_lst + n * 4, 256);
+    const size_t o_flg = o_nt + 128;
+    const size_t total = o_flg + 128;
+    if (cudaMalloc(&e->tables, total) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SF_ERR_OOM, "sf_engine: device tables");
     }
-    if (E.opt.fold_every < 2) E.opt.fold_every = 2;
-    E.opt.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
-    // ---- layout ----
-    E.in.resize(n);
-    int64_t bytes32 = 0, bytes64 = 0, ntiles = 0;
-    for (int b = 0; b < n; ++b) {
-        sf_batch_instance& u = inst[b];
-        SF_REQUIRE(u.Nx >= 4 && u.Ny >= 4 && u.Nx < (1 << 20) && u.Ny < (1 << 20), "sf_solve_stokes_batch_mixed: bad grid");
-        SF_REQUIRE(u.P && u.Vx_pad && u.Vy_pad && u.rho_vy && u.mu_b && u.mu_p && u.Vx_s && u.Vy_s,
-                   "sf_solve_stokes_batch_mixed: NULL array");
-        SF_REQUIRE(u.dx > 0 && u.dy > 0, "sf_solve_stokes_batch_mixed: dx, dy must be positive");
-        HostInst& h = E.in[b];
-        h.user = &u;
-        Inst& I = h.d;
-        memset(&I, 0, sizeof(I));
-        I.Nx = (int)u.Nx;
-        I.Ny = (int)u.Ny;
-        I.ntx = (int)ceil_div(u.Nx - 1, BX);
-        I.nty = (int)ceil_div(u.Ny - 1, BY);
-        I.LD32 = I.LD64 = round_up(u.Nx + 4, 32);
-        I.rows = u.Ny + 3;
-        I.fstride32 = I.fstride64 = I.LD32 * I.rows;
-        h.tile0 = ntiles;
-        h.ntiles = (int64_t)I.ntx * I.nty;
-        ntiles += h.ntiles;
-        bytes32 += (int64_t)G_NUM * I.fstride32 * 4;
-        bytes64 += (int64_t)D_NUM * I.fstride64 * 8;
-        bytes32 = round_up(bytes32, 256);
-        bytes64 = round_up(bytes64, 256);
-    }
-    E.total_tiles = ntiles;
-    // one scratch block: FP32 arena | FP64 arena | maps | insts | tiles | partials | segs | err | list | scale
-    const size_t off32 = 0, off64 = round_up(off32 + bytes32, 256);
-    const size_t offmap = round_up(off64 + bytes64, 256);
-    const size_t offins = round_up(offmap + (size_t)n * M_NUM * sizeof(CUtensorMap), 256);
-    const size_t offtil = round_up(offins + (size_t)n * sizeof(Inst), 256);
-    const size_t offnt = round_up(offtil + (size_t)ntiles * sizeof(int2), 256);
-    const size_t offp32 = round_up(offnt + 256, 256);
-    const size_t offp64 = round_up(offp32 + (size_t)ntiles * 3 * 4, 256);
-    const size_t offseg = round_up(offp64 + (size_t)ntiles * 3 * 8, 256);
-    const size_t offerr = round_up(offseg + (size_t)n * sizeof(Seg), 256);
-    const size_t offlst = round_up(offerr + (size_t)n * 8, 256);
-    const size_t offscl = round_up(offlst + (size_t)n * 4, 256);
-    const size_t total = round_up(offscl + (size_t)n * 8, 256);
-    if ((rc = ensure(ctx, ctx->mixed, total))) return rc;
-    unsigned char* base = (unsigned char*)ctx->mixed.ptr;
-    SF_CUDA(cudaMemsetAsync(base, 0, offmap, s));  // both arenas start at zero (corrections, rates, padding)
-    E.d_maps = (CUtensorMap*)(base + offmap);
-    E.d_insts = (Inst*)(base + offins);
-    E.d_tiles = (int2*)(base + offtil);
-    E.d_ntiles = (int*)(base + offnt);
-    E.d_part64 = (double*)(base + offp64);
-    E.d_segs = (Seg*)(base + offseg);
-    E.d_err = (double*)(base + offerr);
-    E.d_list = (int*)(base + offlst);
-    E.d_scale = (double*)(base + offscl);
-    std::vector<double> h_err_v(n), h_scale(n);
-    // ---- per-instance fields, constants, maps ----
-    std::vector<CUtensorMap> hmaps((size_t)n * M_NUM);
-    int64_t o32 = 0, o64 = 0;
-    const double Vdmp = 4.0, Vsc = 0.45, Ptsc = 0.5;
-    for (int b = 0; b < n; ++b) {
-        HostInst& h = E.in[b];
-        sf_batch_instance& u = *h.user;
-        Inst& I = h.d;
-        I.f32 = (float*)(base + off32 + o32);
-        I.f64 = (double*)(base + off64 + o64);
-        o32 = round_up(o32 + (int64_t)G_NUM * I.fstride32 * 4, 256);
-        o64 = round_up(o64 + (int64_t)D_NUM * I.fstride64 * 8, 256);
-        const int64_t Nx = u.Nx, Ny = u.Ny, LD = I.LD64;
-        const double mdxy = std::min(u.dx, u.dy);
-        I.dx = u.dx;
-        I.dy = u.dy;
-        I._dx = 1.0 / u.dx;
-        I._dy = 1.0 / u.dy;
-        I.g_y = u.g_y;
-        I.maxdisp = u.maxdisp;
-        I.use_stab = u.use_free_surface_stabilization ? 1 : 0;
-        I.dt_in = I.use_stab ? u.dt : 0.0;
-        I.dt = I.dt_in;
-        I._dxf = (float)I._dx;
-        I._dyf = (float)I._dy;
-        I.dampXf = (float)(1.0 - Vdmp / (double)Nx);
-        I.dampYf = (float)(1.0 - Vdmp / (double)Ny);
-        I.c_vscf = (float)(Vsc * mdxy * mdxy / 4.1);
-        I.c_ptscf = (float)(Ptsc * 4.1 / (double)std::max(Nx, Ny));
-        I.g_dtf = (float)(I.g_y * I.dt);
-        // pack the caller's FP64 arrays
-        double* f64 = I.f64;
-        struct Pk { int f; const double* src; int64_t nx, ny; } packs[] = {
-            {D_VX, u.Vx_s, Nx, Ny + 1}, {D_VY, u.Vy_s, Nx + 1, Ny}, {D_P, u.P, Nx - 1, Ny - 1},
-            {D_RHO, u.rho_vy, Nx + 1, Ny}, {D_MUB, u.mu_b, Nx, Ny}, {D_MUP, u.mu_p, Nx - 1, Ny - 1}};
-        for (const Pk& k : packs) {
-            k_copy64<<<grid1(k.nx * k.ny, 256), 256, 0, s>>>(f64 + (int64_t)k.f * I.fstride64, LD, k.src, k.nx, k.nx, k.ny);
-            SF_LAUNCHED(ctx);
-        }
-        struct Cv { int g, d; int64_t nx, ny; } cvs[] = {{G_MUB, D_MUB, Nx, Ny}, {G_MUP, D_MUP, Nx - 1, Ny - 1},
-                                                           {G_RHO, D_RHO, Nx + 1, Ny}};
-        for (const Cv& c : cvs) {
-            k_f64_to_f32<<<grid1(c.nx * c.ny, 256), 256, 0, s>>>(I.f32 + (int64_t)c.g * I.fstride32, LD,
-                                                                 f64 + (int64_t)c.d * I.fstride64, LD, c.nx, c.ny);
-            SF_LAUNCHED(ctx);
-        }
-        if (u.rel_tol > 0) {
-            k_rho_scale64<<<1, 1024, 0, s>>>(u.rho_vy, (int)Nx, (int)Ny, u.g_y, E.d_scale + b);
-            SF_LAUNCHED(ctx);
-        }
-        // tensor maps (FP32 fields, LD x rows)
-        const int gmap[M_NUM] = {G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_MUB, G_MUP, G_RHO, G_RDIV,
-                                 G_RVX, G_RVY, G_RX, G_RY};
-        for (int m = 0; m < M_NUM; ++m) {
-            const bool halo = m <= M_RDIV;
-            if ((rc = encode_tmap_f32(&hmaps[(size_t)b * M_NUM + m], I.f32 + (int64_t)gmap[m] * I.fstride32, LD,
-                                      I.rows, halo ? TW : BX, halo ? TH : BY)))
-                return rc;
-        }
-    }
-    SF_CUDA(cudaMemcpyAsync(E.d_maps, hmaps.data(), hmaps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s));
-    SF_CUDA(cudaMemcpyAsync(h_scale.data(), E.d_scale, (size_t)n * 8, cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaStreamSynchronize(s));
-    for (int b = 0; b < n; ++b) {
-        HostInst& h = E.in[b];
-        h.eps = h.user->rel_tol > 0 ? h.user->rel_tol * h_scale[b] : h.user->eps;
-        if ((rc = E.upload_inst(b))) return rc;
-    }
+    unsigned char* b = (unsigned char*)e->tables;
+    e->d_insts = (Inst*)(b + o_ins);
+    e->d_maps = (CUtensorMap*)(b + o_map);
+    e->d_segs = (Seg*)(b + o_seg);
+    e->d_out = (double*)(b + o_out);
+    e->d_scale = (double*)(b + o_scl);
+    e->d_list = (int*)(b + o_lst);
+    e->d_ntiles = (int*)(b + o_nt);
+    e->d_flag = (int*)(b + o_flg);
+    SF_CUDA(cudaMemsetAsync(e->tables, 0, total, e->s));
+    SF_CUDA(cudaMallocHost(&e->h_out, n * 3 * 8 + 64));  // {err, scale, dt_cfl} per slot, then the flag word
+    e->slots.assign(n, Slot{});
+    e->free_slots.clear();
+    for (int k = slot_cap - 1; k >= 0; --k) e->free_slots.push_back(k);
     static int per_sm = 0;
     if (!per_sm) {
         SF_CUDA(cudaFuncSetAttribute(k_pt32, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
         SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt32, NT, SMEM_BYTES));
         if (per_sm < 1) return fail(SF_ERR_CUDA, "k_pt32 does not fit on an SM");
     }
-    SF_CUDA(cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), s));
-    std::vector<int2> h_tiles((size_t)ntiles);
-    std::vector<Seg> h_segs(n);
-    std::vector<int> ids;
-    ids.reserve(n);
-    cudaEvent_t e0 = ctx->ev_a, e1 = ctx->ev_b;
-    SF_CUDA(cudaEventRecord(e0, s));
-
-    // ---- the loop: an outer step (fold the correction into V, P -> dt -> FP64 residual) for every
-    // instance still iterating, then K FP32 sweeps of all of them.  K is even, so each instance's
-    // current correction stays in its A buffers at every fold (no buffer bookkeeping). ----
-    const int K = E.opt.fold_every;
-    const int blocks = (int)std::min<int64_t>(E.total_tiles, (int64_t)per_sm * ctx->num_sms);
-    std::vector<int> sweep_ids_prev;
-    bool first = true;
-    while (true) {
-        ids.clear();
-        for (int b = 0; b < n; ++b)
-            if (E.in[b].phase != PH_DONE) ids.push_back(b);
-        if (ids.empty()) break;
-        int64_t nt = 0;
-        if (!first) {
-            // fold: V += dV, P += dP for every instance that just swept
-            SF_CUDA(cudaMemcpyAsync(E.d_list, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, s));
-            k_accumulate<<<dim3(64, (unsigned)ids.size()), 256, 0, s>>>(E.d_insts, E.d_list, 0);
-            SF_LAUNCHED(ctx);
-        }
-        E.build_lists(ids, h_tiles.data(), h_segs.data(), &nt);
-        SF_CUDA(cudaMemcpyAsync(E.d_tiles, h_tiles.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, s));
-        SF_CUDA(cudaMemcpyAsync(E.d_segs, h_segs.data(), ids.size() * sizeof(Seg), cudaMemcpyHostToDevice, s));
-        E.h_ntiles = (int)nt;
-        SF_CUDA(cudaMemcpyAsync(E.d_ntiles, &E.h_ntiles, sizeof(int), cudaMemcpyHostToDevice, s));
-        k_maxv64<<<(unsigned)nt, T64, 0, s>>>(E.d_insts, E.d_tiles, E.d_part64);
-        SF_LAUNCHED(ctx);
-        k_inst_dt<<<(unsigned)ids.size(), 256, 0, s>>>(E.d_insts, E.d_segs, E.d_part64);
-        SF_LAUNCHED(ctx);
-        k_resid64<<<(unsigned)nt, T64, 0, s>>>(E.d_insts, E.d_tiles, E.d_part64);
-        SF_LAUNCHED(ctx);
-        k_inst_err<<<(unsigned)ids.size(), 256, 0, s>>>(E.d_segs, E.d_part64, E.d_insts, E.d_err);
-        SF_LAUNCHED(ctx);
-        SF_CUDA(cudaMemcpyAsync(h_err_v.data(), E.d_err, ids.size() * 8, cudaMemcpyDeviceToHost, s));
-        SF_CUDA(cudaStreamSynchronize(s));
-        int flag = 0;
-        SF_CUDA(cudaMemcpy(&flag, ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
-        if (flag) return fail(SF_ERR_CUDA, "sf_solve_stokes_batch_mixed: a tile copy did not complete in time");
-        first = false;
-        std::vector<int> sweep;
-        for (size_t q = 0; q < ids.size(); ++q) {
-            HostInst& h = E.in[ids[q]];
-            h.err = h_err_v[q];
-            ++h.outer;
-            const bool bad = !(h.err == h.err) || std::isinf(h.err);
-            if (bad || h.err <= h.eps || h.inner_total >= E.opt.max_sweeps)
-                h.phase = PH_DONE;
-            else
-                sweep.push_back(ids[q]);
-        }
-        if (sweep.empty()) continue;
-        if (sweep != ids) {
-            E.build_lists(sweep, h_tiles.data(), h_segs.data(), &nt);
-            SF_CUDA(cudaMemcpyAsync(E.d_tiles, h_tiles.data(), nt * sizeof(int2), cudaMemcpyHostToDevice, s));
-            E.h_ntiles = (int)nt;
-            SF_CUDA(cudaMemcpyAsync(E.d_ntiles, &E.h_ntiles, sizeof(int), cudaMemcpyHostToDevice, s));
-        }
-        auto launch_run = [&]() -> int {
-            for (int k = 0; k < K; ++k) {
-                k_pt32<<<blocks, dim3(BX, TY), SMEM_BYTES, s>>>(E.d_maps, E.d_insts, E.d_tiles, E.d_ntiles, k & 1,
-                                                                ctx->d_flags);
-                SF_CHECK_LAUNCH();
-            }
-            return SF_OK;
-        };
-        if (E.opt.use_graphs) {
-            if (!E.gexec) {
-                SF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-                int lrc = launch_run();
-                cudaGraph_t g = nullptr;
-                cudaError_t ce = cudaStreamEndCapture(s, &g);
-                if (lrc) return lrc;
-                SF_CUDA(ce);
-                E.graph = g;
-                SF_CUDA(cudaGraphInstantiate(&E.gexec, g, 0));
-            }
-            SF_CUDA(cudaGraphLaunch(E.gexec, s));
-        } else {
-            if ((rc = launch_run())) return rc;
-        }
-        ctx->launches += K;
-        E.launches += K;
-        for (int b : sweep) E.in[b].inner_total += K;
-    }
-    SF_CUDA(cudaEventRecord(e1, s));
-    // the device-side instance records hold the last dt computed from the FP64 velocities
-    std::vector<Inst> dev_inst(n);
-    SF_CUDA(cudaMemcpyAsync(dev_inst.data(), E.d_insts, (size_t)n * sizeof(Inst), cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaStreamSynchronize(s));
-    for (int b = 0; b < n; ++b) E.in[b].d.dt_cfl = dev_inst[b].dt_cfl;
-    // ---- unpack (:89-95) ----
-    for (int b = 0; b < n; ++b) {
-        HostInst& h = E.in[b];
-        sf_batch_instance& u = *h.user;
-        const Inst& I = h.d;
-        const int64_t Nx = u.Nx, Ny = u.Ny, LD = I.LD64;
-        struct Uk { double* dst; int f; int64_t nx, ny; } ups[] = {
-            {u.Vx_s, D_VX, Nx, Ny + 1}, {u.Vy_s, D_VY, Nx + 1, Ny}, {u.P, D_P, Nx - 1, Ny - 1}};
-        for (const Uk& k : ups) {
-            k_copy64<<<grid1(k.nx * k.ny, 256), 256, 0, s>>>(k.dst, k.nx, I.f64 + (int64_t)k.f * I.fstride64, LD, k.nx, k.ny);
-            SF_LAUNCHED(ctx);
-        }
-        k_pad_vx64<<<grid1((Nx + 2) * (Ny + 1), 256), 256, 0, s>>>(u.Vx_pad, I.f64 + D_VX * I.fstride64, LD, (int)Nx, (int)Ny);
-        SF_LAUNCHED(ctx);
-        k_pad_vy64<<<grid1((Nx + 1) * (Ny + 2), 256), 256, 0, s>>>(u.Vy_pad, I.f64 + D_VY * I.fstride64, LD, (int)Nx, (int)Ny);
-        SF_LAUNCHED(ctx);
-        u.dt_out = I.dt_cfl;   // compute_dt of the final V (:95), from the last outer step
-        u.err = h.err;
-        u.inner_iters = h.inner_total;
-        u.outer_iters = h.outer;
-        u.converged = (h.err <= h.eps) ? 1 : 0;
-        u.eps_used = h.eps;
-        u.status = (h.err == h.err && !std::isinf(h.err)) ? SF_OK : SF_ERR_NONFINITE;
-    }
-    SF_CUDA(cudaStreamSynchronize(s));
-    float ms = 0.f;
-    SF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    for (int b = 0; b < n; ++b) inst[b].batch_ms = ms;
+    e->blocks = per_sm * ctx->num_sms;  // persistent: one wave; CTAs beyond the tile count exit at once
     return SF_OK;
 }
 
+int ensure_tiles(sf_engine* e, int64_t need) {
+    if (need <= e->tile_cap) return SF_OK;
+    const int64_t cap = std::max<int64_t>({need, 2 * e->tile_cap, 4096});
+    SF_CUDA(cudaStreamSynchronize(e->s));  // the old lists may still be read by queued sweeps
+    drop_graph(e);                         // the graph holds the old pointer
+    if (e->d_tiles) cudaFree(e->d_tiles);
+    if (e->d_part) cudaFree(e->d_part);
+    e->d_tiles = nullptr;
+    e->d_part = nullptr;
+    e->tile_cap = 0;
+    if (cudaMalloc(&e->d_tiles, (size_t)cap * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&e->d_part, (size_t)cap * 3 * 8) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SF_ERR_OOM, "sf_engine: tile list");
+    }
+    e->tile_cap = cap;
+    e->h_tiles.resize((size_t)cap);
+    return SF_OK;
+}
+
+// tile list + segments of the slots in `ids` -> device; returns the tile count in *nt
+int upload_lists(sf_engine* e, const std::vector<int>& ids, bool segs, int64_t* nt_out) {
+    int64_t nt = 0;
+    for (int q : ids) nt += e->slots[q].ntiles;
+    int rc = ensure_tiles(e, nt);
+    if (rc) return rc;
+    if (segs) e->h_segs.resize(ids.size());
+    int64_t k = 0;
+    for (size_t q = 0; q < ids.size(); ++q) {
+        const Slot& h = e->slots[ids[q]];
+        if (segs) e->h_segs[q] = Seg{ids[q], (int)k, (int)(k + h.ntiles), 0};
+        for (int64_t t = 0; t < h.ntiles; ++t) e->h_tiles[k++] = make_int2(ids[q], (int)t);
+    }
+    // pageable sources: the copies are staged before cudaMemcpyAsync returns, so the host vectors are free again
+    SF_CUDA(cudaMemcpyAsync(e->d_tiles, e->h_tiles.data(), (size_t)nt * sizeof(int2), cudaMemcpyHostToDevice, e->s));
+    if (segs)
+        SF_CUDA(cudaMemcpyAsync(e->d_segs, e->h_segs.data(), ids.size() * sizeof(Seg), cudaMemcpyHostToDevice, e->s));
+    e->h_ntiles = (int)nt;
+    SF_CUDA(cudaMemcpyAsync(e->d_ntiles, &e->h_ntiles, sizeof(int), cudaMemcpyHostToDevice, e->s));
+    *nt_out = nt;
+    return SF_OK;
+}
+
+int launch_sweeps(sf_engine* e) {
+    const int K = e->opt.fold_every;
+    auto run = [&]() -> int {
+        for (int k = 0; k < K; ++k) {
+            k_pt32<<<e->blocks, dim3(BX, TY), SMEM_BYTES, e->s>>>(e->d_maps, e->d_insts, e->d_tiles, e->d_ntiles,
+                                                                   k & 1, e->d_flag);
+            SF_CHECK_LAUNCH();
+        }
+        return SF_OK;
+    };
+    if (e->opt.use_graphs) {
+        if (e->gexec && e->graph_k != K) drop_graph(e);
+        if (!e->gexec) {
+            SF_CUDA(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
+            int lrc = run();
+            cudaGraph_t g = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(e->s, &g);
+            if (lrc) {
+                if (g) cudaGraphDestroy(g);
+                return lrc;
+            }
+            SF_CUDA(ce);
+            e->graph = g;
+            SF_CUDA(cudaGraphInstantiate(&e->gexec, g, 0));
+            e->graph_k = K;
+        }
+        SF_CUDA(cudaGraphLaunch(e->gexec, e->s));
+    } else {
+        int rc = run();
+        if (rc) return rc;
+    }
+    e->ctx->launches += K;
+    e->sweeps += K;
+    return SF_OK;
+}
+
+// packs the caller's arrays of slot q into the arena and fills its device record and tensor maps
+int admit(sf_engine* e, int q, sf_batch_instance& u) {
+    sf_ctx* ctx = e->ctx;
+    cudaStream_t s = e->s;
+    Slot& h = e->slots[q];
+    Inst& I = h.d;
+    memset(&I, 0, sizeof(I));
+    const Layout L(u.Nx, u.Ny);
+    I.Nx = (int)u.Nx;
+    I.Ny = (int)u.Ny;
+    I.ntx = (int)ceil_div(u.Nx - 1, BX);
+    I.nty = (int)ceil_div(u.Ny - 1, BY);
+    I.LD32 = I.LD64 = L.LD;
+    I.rows = L.rows;
+    I.fstride32 = I.fstride64 = L.fstride;
+    I.f32 = (float*)(e->arena + h.off);
+    I.f64 = (double*)(e->arena + h.off + L.bytes32);
+    h.ntiles = (int64_t)I.ntx * I.nty;
+    const double Vdmp = 4.0, Vsc = 0.45, Ptsc = 0.5;  // StokesSolver_multixpu.jl:17-19
+    const int64_t Nx = u.Nx, Ny = u.Ny, LD = L.LD;
+    const double mdxy = std::min(u.dx, u.dy);
+    I.dx = u.dx;
+    I.dy = u.dy;
+    I._dx = 1.0 / u.dx;
+    I._dy = 1.0 / u.dy;
+    I.g_y = u.g_y;
+    I.maxdisp = u.maxdisp;
+    I.use_stab = u.use_free_surface_stabilization ? 1 : 0;
+    I.dtau_max = e->opt.dtau_local_max ? 1 : 0;
+    I.dt_in = I.use_stab ? u.dt : 0.0;
+    I.dt = I.dt_in;
+    I._dxf = (float)I._dx;
+    I._dyf = (float)I._dy;
+    I.dampXf = (float)(1.0 - Vdmp / (double)Nx);
+    I.dampYf = (float)(1.0 - Vdmp / (double)Ny);
+    I.c_vscf = (float)(Vsc * mdxy * mdxy / 4.1);
+    I.c_ptscf = (float)(Ptsc * 4.1 / (double)std::max(Nx, Ny));
+    I.g_dtf = (float)(I.g_y * I.dt);
+    // corrections, rates and every padding entry start at zero
+    SF_CUDA(cudaMemsetAsync(e->arena + h.off, 0, (size_t)h.bytes, s));
+    double* f64 = I.f64;
+    struct Pk { int f; const double* src; int64_t nx, ny; } packs[] = {
+        {D_VX, u.Vx_s, Nx, Ny + 1}, {D_VY, u.Vy_s, Nx + 1, Ny}, {D_P, u.P, Nx - 1, Ny - 1},
+        {D_RHO, u.rho_vy, Nx + 1, Ny}, {D_MUB, u.mu_b, Nx, Ny}, {D_MUP, u.mu_p, Nx - 1, Ny - 1}};
+    for (const Pk& k : packs) {
+        k_copy64<<<grid1(k.nx * k.ny, 256), 256, 0, s>>>(f64 + (int64_t)k.f * I.fstride64, LD, k.src, k.nx, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    struct Cv { int g, d; int64_t nx, ny; } cvs[] = {{G_MUB, D_MUB, Nx, Ny}, {G_MUP, D_MUP, Nx - 1, Ny - 1},
+                                                       {G_RHO, D_RHO, Nx + 1, Ny}};
+    for (const Cv& c : cvs) {
+        k_f64_to_f32<<<grid1(c.nx * c.ny, 256), 256, 0, s>>>(I.f32 + (int64_t)c.g * I.fstride32, LD,
+                                                             f64 + (int64_t)c.d * I.fstride64, LD, c.nx, c.ny);
+        SF_LAUNCHED(ctx);
+    }
+    if (u.rel_tol > 0) {
+        k_rho_scale64<<<1, 1024, 0, s>>>(u.rho_vy, (int)Nx, (int)Ny, u.g_y, e->d_scale + q);
+        SF_LAUNCHED(ctx);
+    }
+    CUtensorMap maps[M_NUM];
+    const int gmap[M_NUM] = {G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_MUB, G_MUP, G_RHO, G_RDIV,
+                             G_RVX, G_RVY, G_RX, G_RY};
+    for (int m = 0; m < M_NUM; ++m) {
+        const bool halo = m <= M_RDIV;
+        int rc = encode_tmap_f32(&maps[m], I.f32 + (int64_t)gmap[m] * I.fstride32, LD, I.rows, halo ? TW : BX,
+                                 halo ? TH : BY);
+        if (rc) return rc;
+    }
+    SF_CUDA(cudaMemcpyAsync(e->d_maps + (size_t)q * M_NUM, maps, sizeof(maps), cudaMemcpyHostToDevice, s));
+    SF_CUDA(cudaMemcpyAsync(e->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, s));
+    return SF_OK;
+}
+
+// writes the FP64 state of slot q back to the caller's arrays (:89-95) and its results into the struct
+int write_back(sf_engine* e, int q, double dt_cfl) {
+    sf_ctx* ctx = e->ctx;
+    cudaStream_t s = e->s;
+    Slot& h = e->slots[q];
+    sf_batch_instance& u = *h.user;
+    const Inst& I = h.d;
+    const int64_t Nx = u.Nx, Ny = u.Ny, LD = I.LD64;
+    struct Uk { double* dst; int f; int64_t nx, ny; } ups[] = {
+        {u.Vx_s, D_VX, Nx, Ny + 1}, {u.Vy_s, D_VY, Nx + 1, Ny}, {u.P, D_P, Nx - 1, Ny - 1}};
+    for (const Uk& k : ups) {
+        k_copy64<<<grid1(k.nx * k.ny, 256), 256, 0, s>>>(k.dst, k.nx, I.f64 + (int64_t)k.f * I.fstride64, LD, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    k_pad_vx64<<<grid1((Nx + 2) * (Ny + 1), 256), 256, 0, s>>>(u.Vx_pad, I.f64 + D_VX * I.fstride64, LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    k_pad_vy64<<<grid1((Nx + 1) * (Ny + 2), 256), 256, 0, s>>>(u.Vy_pad, I.f64 + D_VY * I.fstride64, LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    u.dt_out = dt_cfl;  // compute_dt of the final V (:95), from the last outer step
+    u.err = h.err;
+    u.inner_iters = h.inner_total;
+    u.outer_iters = h.outer;
+    u.converged = (h.err <= h.eps) ? 1 : 0;
+    u.eps_used = h.eps;
+    u.status = (h.err == h.err && !std::isinf(h.err)) ? SF_OK : SF_ERR_NONFINITE;
+    u.batch_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h.t_submit).count();
+    return SF_OK;
+}
+
+int validate(const sf_batch_instance& u, const char* who) {
+    const std::string w(who);
+    SF_REQUIRE(u.Nx >= 4 && u.Ny >= 4 && u.Nx < (1 << 20) && u.Ny < (1 << 20), (w + ": bad grid").c_str());
+    SF_REQUIRE(u.P && u.Vx_pad && u.Vy_pad && u.rho_vy && u.mu_b && u.mu_p && u.Vx_s && u.Vy_s,
+               (w + ": NULL array").c_str());
+    SF_REQUIRE(u.dx > 0 && u.dy > 0, (w + ": dx, dy must be positive").c_str());
+    return SF_OK;
+}
+
+int engine_submit(sf_engine* e, sf_batch_instance* u, cudaStream_t caller, int64_t* ticket) {
+    int rc = validate(*u, "sf_engine_submit");
+    if (rc) return rc;
+    const int64_t bytes = Layout(u->Nx, u->Ny).bytes();
+    if (bytes > e->alloc.cap())
+        return fail(SF_ERR_TOO_LARGE, "sf_engine_submit: the instance needs " + std::to_string(bytes) +
+                                          " arena bytes, more than the engine has");
+    if (e->free_slots.empty()) return fail(SF_ERR_BUSY, "sf_engine_submit: instance table full");
+    const int64_t off = e->alloc.alloc(bytes);
+    if (off < 0) return fail(SF_ERR_BUSY, "sf_engine_submit: arena full");
+    const int q = e->free_slots.back();
+    e->free_slots.pop_back();
+    Slot& h = e->slots[q];
+    h = Slot{};
+    h.user = u;
+    h.off = off;
+    h.bytes = bytes;
+    h.t_submit = std::chrono::steady_clock::now();
+    // the inputs are ready once the work queued on the caller's stream is done
+    SF_CUDA(cudaEventRecord(e->ev_in, caller));
+    SF_CUDA(cudaStreamWaitEvent(e->s, e->ev_in, 0));
+    if ((rc = admit(e, q, *u))) {
+        e->alloc.release(off, bytes);
+        e->free_slots.push_back(q);
+        return rc;
+    }
+    h.active = true;
+    h.ticket = e->next_ticket++;
+    ++e->submitted;
+    if (ticket) *ticket = h.ticket;
+    return SF_OK;
+}
+
+// one round: fold -> dt -> FP64 residual -> stopping test -> write-back of the finished -> sweeps of the rest
+int engine_round(sf_engine* e, cudaStream_t caller) {
+    sf_ctx* ctx = e->ctx;
+    cudaStream_t s = e->s;
+    std::vector<int> ids, swept;
+    for (int q = 0; q < (int)e->slots.size(); ++q)
+        if (e->slots[q].active) {
+            ids.push_back(q);
+            if (e->slots[q].swept) swept.push_back(q);
+        }
+    if (ids.empty()) return SF_OK;
+    ++e->rounds;
+    int rc;
+    if (!swept.empty()) {  // V += dV, P += dP for every instance that ran sweeps
+        SF_CUDA(cudaMemcpyAsync(e->d_list, swept.data(), swept.size() * 4, cudaMemcpyHostToDevice, s));
+        k_accumulate<<<dim3(64, (unsigned)swept.size()), 256, 0, s>>>(e->d_insts, e->d_list, 0);
+        SF_LAUNCHED(ctx);
+    }
+    int64_t nt = 0;
+    if ((rc = upload_lists(e, ids, true, &nt))) return rc;
+    k_maxv64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles, e->d_part);
+    SF_LAUNCHED(ctx);
+    k_inst_dt<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_insts, e->d_segs, e->d_part);
+    SF_LAUNCHED(ctx);
+    k_resid64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles, e->d_part);
+    SF_LAUNCHED(ctx);
+    k_inst_err<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_segs, e->d_part, e->d_insts, e->d_scale, e->d_out);
+    SF_LAUNCHED(ctx);
+    SF_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, ids.size() * 3 * 8, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(e->h_out + ids.size() * 3, e->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    int flag = 0;
+    memcpy(&flag, e->h_out + ids.size() * 3, sizeof(int));
+    if (flag) return fail(SF_ERR_CUDA, "sf_engine: a tile copy did not complete in time");
+    std::vector<int> sweep;
+    bool any_done = false;
+    for (size_t k = 0; k < ids.size(); ++k) {
+        const int q = ids[k];
+        Slot& h = e->slots[q];
+        h.err = e->h_out[3 * k];
+        if (h.outer == 0) h.eps = h.user->rel_tol > 0 ? h.user->rel_tol * e->h_out[3 * k + 1] : h.user->eps;
+        ++h.outer;
+        h.swept = false;
+        const bool bad = !(h.err == h.err) || std::isinf(h.err);
+        if (bad || h.err <= h.eps || h.inner_total >= e->opt.max_sweeps) {
+            if ((rc = write_back(e, q, e->h_out[3 * k + 2]))) return rc;
+            h.active = false;
+            e->alloc.release(h.off, h.bytes);
+            e->free_slots.push_back(q);
+            e->pending.push_back(h.ticket);
+            ++e->finished;
+            any_done = true;
+        } else {
+            sweep.push_back(q);
+        }
+    }
+    if (any_done) {  // the caller's later work sees the written-back arrays
+        SF_CUDA(cudaEventRecord(e->ev_out, s));
+        SF_CUDA(cudaStreamWaitEvent(caller, e->ev_out, 0));
+    }
+    if (sweep.empty()) return SF_OK;
+    if (sweep.size() != ids.size() && (rc = upload_lists(e, sweep, false, &nt))) return rc;
+    if ((rc = launch_sweeps(e))) return rc;
+    for (int q : sweep) {
+        e->slots[q].inner_total += e->opt.fold_every;
+        e->slots[q].swept = true;
+    }
+    return SF_OK;
+}
+
+int active_count(const sf_engine* e) {
+    int n = 0;
+    for (const Slot& h : e->slots) n += h.active ? 1 : 0;
+    return n;
+}
+
+}  // namespace
+
+void sf::mixed_engine_release(sf_ctx* ctx) {
+    if (ctx && ctx->batch_engine) {
+        engine_free(ctx->batch_engine);
+        ctx->batch_engine = nullptr;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: engine
+// ---------------------------------------------------------------------------
+extern "C" int sf_engine_instance_bytes(int64_t Nx, int64_t Ny, int64_t* bytes) {
+    SF_REQUIRE(bytes && Nx >= 4 && Ny >= 4 && Nx < (1 << 20) && Ny < (1 << 20), "sf_engine_instance_bytes: bad arguments");
+    *bytes = Layout(Nx, Ny).bytes();
+    return SF_OK;
+}
+
+extern "C" int sf_engine_create(sf_ctx* ctx, int64_t arena_bytes, int32_t max_instances, const sf_mixed_options* opt,
+                                sf_engine** out) {
+    SF_REQUIRE(ctx && out && arena_bytes > 0 && max_instances >= 1, "sf_engine_create: bad arguments");
+    *out = nullptr;
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    sf_engine* e = new sf_engine();
+    if ((rc = engine_init(e, ctx, max_instances, opt))) {
+        engine_free(e);
+        return rc;
+    }
+    const int64_t cap = round_up(arena_bytes, 256);
+    if (cudaMalloc(&e->arena, (size_t)cap) != cudaSuccess) {
+        cudaGetLastError();
+        e->arena = nullptr;
+        engine_free(e);
+        return fail(SF_ERR_OOM, "sf_engine_create: arena of " + std::to_string(cap) + " bytes");
+    }
+    e->arena_owned = true;
+    e->alloc.reset(cap);
+    *out = e;
+    return SF_OK;
+}
+
+extern "C" int sf_engine_destroy(sf_engine* e) {
+    if (!e) return SF_OK;
+    cudaSetDevice(e->ctx->device);
+    engine_free(e);
+    return SF_OK;
+}
+
+extern "C" int sf_engine_submit(sf_engine* e, sf_batch_instance* inst, void* stream, int64_t* ticket) {
+    SF_REQUIRE(e && inst, "sf_engine_submit: NULL argument");
+    int rc = set_device(e->ctx);
+    if (rc) return rc;
+    return engine_submit(e, inst, as_stream(stream), ticket);
+}
+
+extern "C" int sf_engine_step(sf_engine* e, void* stream, int64_t* finished, int32_t cap, int32_t* n_finished,
+                              int32_t* n_active) {
+    SF_REQUIRE(e && (cap <= 0 || finished), "sf_engine_step: bad arguments");
+    int rc = set_device(e->ctx);
+    if (rc) return rc;
+    if ((rc = engine_round(e, as_stream(stream)))) return rc;
+    int32_t k = 0;
+    while (k < cap && !e->pending.empty()) {
+        finished[k++] = e->pending.front();
+        e->pending.pop_front();
+    }
+    if (n_finished) *n_finished = k;
+    if (n_active) *n_active = active_count(e);
+    return SF_OK;
+}
+
+extern "C" int sf_engine_get_stats(sf_engine* e, sf_engine_stats* st) {
+    SF_REQUIRE(e && st, "sf_engine_get_stats: NULL argument");
+    memset(st, 0, sizeof(*st));
+    st->arena_bytes = e->alloc.cap();
+    st->arena_used = e->alloc.used();
+    st->arena_peak = e->alloc.peak();
+    st->submitted = e->submitted;
+    st->finished = e->finished;
+    st->rounds = e->rounds;
+    st->sweeps = e->sweeps;
+    st->active = active_count(e);
+    st->pending_results = (int32_t)e->pending.size();
+    return SF_OK;
+}
+
+extern "C" int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst, int n, const sf_mixed_options* o,
+                                           void* stream) {
+    SF_REQUIRE(ctx && inst && n >= 1, "sf_solve_stokes_batch_mixed: bad arguments");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    int64_t total = 0;
+    for (int b = 0; b < n; ++b) {
+        if ((rc = validate(inst[b], "sf_solve_stokes_batch_mixed"))) return rc;
+        total += Layout(inst[b].Nx, inst[b].Ny).bytes();
+    }
+    // the context keeps one engine for this call (tables, graph); its arena is the context's scratch,
+    // sized to the batch, so every instance is admitted at once
+    sf_engine* e = ctx->batch_engine;
+    if (e && (int)e->slots.size() < n) {
+        mixed_engine_release(ctx);
+        e = nullptr;
+    }
+    if (!e) {
+        e = new sf_engine();
+        if ((rc = engine_init(e, ctx, std::max(n, 64), o))) {
+            engine_free(e);
+            return rc;
+        }
+        ctx->batch_engine = e;
+    }
+    e->opt = normalized(o);
+    if ((rc = ensure(ctx, ctx->mixed, (size_t)total))) return rc;
+    e->arena = (unsigned char*)ctx->mixed.ptr;
+    e->alloc.reset(total);
+    auto run = [&]() -> int {
+        int r;
+        cudaStream_t caller = as_stream(stream);
+        SF_CUDA(cudaEventRecord(ctx->ev_a, caller));
+        SF_CUDA(cudaStreamWaitEvent(e->s, ctx->ev_a, 0));
+        SF_CUDA(cudaEventRecord(ctx->ev_b, e->s));
+        for (int b = 0; b < n; ++b)
+            if ((r = engine_submit(e, &inst[b], caller, nullptr))) return r;
+        while (active_count(e) > 0)
+            if ((r = engine_round(e, caller))) return r;
+        e->pending.clear();
+        SF_CUDA(cudaEventRecord(ctx->ev_c, e->s));
+        SF_CUDA(cudaStreamSynchronize(e->s));
+        float ms = 0.f;
+        SF_CUDA(cudaEventElapsedTime(&ms, ctx->ev_b, ctx->ev_c));
+        for (int b = 0; b < n; ++b) inst[b].batch_ms = ms;
+        return SF_OK;
+    };
+    if ((rc = run())) {
+        mixed_engine_release(ctx);  // its state is unknown after an error
+        return rc;
+    }
+    return SF_OK;
+}
 extern "C" int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy,
                                      const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s, double g_y,
                                      double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,

@@ -21,6 +21,7 @@ SF_ERR_OOM = 3
 SF_ERR_NO_DEVICE = 4
 SF_ERR_NONFINITE = 5
 SF_ERR_TOO_LARGE = 6
+SF_ERR_BUSY = 7
 
 # limits of the allocation-free deposit (include/stokesflow_b200.h)
 SF_NOALLOC_MAX_MARKERS = 1048576
@@ -68,7 +69,17 @@ class BatchInstance(C.Structure):
 
 class MixedOptions(C.Structure):
     """sf_mixed_options."""
-    _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32)]
+    _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32), ("dtau_local_max", _i32),
+                ("reserved", _i32)]
+
+
+class EngineStats(C.Structure):
+    """sf_engine_stats."""
+    _fields_ = [("arena_bytes", _i64), ("arena_used", _i64), ("arena_peak", _i64), ("submitted", _i64),
+                ("finished", _i64), ("rounds", _i64), ("sweeps", _i64), ("active", _i32), ("pending_results", _i32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class PlumeModelC(C.Structure):
@@ -96,6 +107,12 @@ PROTOTYPES = {
     "sf_solve_stokes_batch_mixed": (C.c_int, [_vp, C.POINTER(BatchInstance), C.c_int, C.POINTER(MixedOptions), _vp]),
     "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64, _d, _d,
                                         C.c_int, _d, _d, C.POINTER(MixedOptions), _vp, C.POINTER(BatchInstance)]),
+    "sf_engine_instance_bytes": (C.c_int, [_i64, _i64, C.POINTER(_i64)]),
+    "sf_engine_create": (C.c_int, [_vp, _i64, _i32, C.POINTER(MixedOptions), C.POINTER(_vp)]),
+    "sf_engine_destroy": (C.c_int, [_vp]),
+    "sf_engine_submit": (C.c_int, [_vp, C.POINTER(BatchInstance), _vp, C.POINTER(_i64)]),
+    "sf_engine_step": (C.c_int, [_vp, _vp, C.POINTER(_i64), _i32, C.POINTER(_i32), C.POINTER(_i32)]),
+    "sf_engine_get_stats": (C.c_int, [_vp, C.POINTER(EngineStats)]),
     "sf_move_markers_rk4": (C.c_int, [_vp, _pd, _pd, _i64, _pd, _i64, _i64, _pd, _i64, _i64, _d, _d, _d, _d, _d, _d,
                                       _d, _d, _d, _vp]),
     "sf_rebin_markers": (C.c_int, [_vp, _pd, _pd, _i64, _d, _d, _d, _d, _i64, _i64, _pd, _pd, _pd, _vp]),

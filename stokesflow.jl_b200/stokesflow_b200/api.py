@@ -35,7 +35,8 @@ from ._lib import check, lib
 
 __all__ = ["Context", "default_context", "zeros", "bilinear_marker_to_grid", "solve_stokes", "solve_stokes_info",
            "residual_scale", "move_markers_rk4", "rebin_markers", "marker_count", "initialize_markers",
-           "initialize_markers_host", "set_initial_marker_properties", "get_warnings", "PlumeModel"]
+           "initialize_markers_host", "set_initial_marker_properties", "get_warnings", "PlumeModel", "MixedProblem",
+           "mixed_options", "solve_stokes_batch_mixed", "Engine", "bilinear_marker_to_grid_noalloc"]
 
 
 class Context:
@@ -229,9 +230,11 @@ class MixedProblem:
         self.result = None
 
 
-def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True):
-    """Options of the mixed-precision / batched solver (sf_mixed_options)."""
-    return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)))
+def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True, dtau_local_max=False):
+    """Options of the mixed-precision / batched solver (sf_mixed_options).  dtau_local_max: pseudo-time
+    steps from the stencil's largest viscosity instead of the reference's average (faster on soft
+    inclusions); the converged solution is the same."""
+    return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)), int(bool(dtau_local_max)), 0)
 
 
 def solve_stokes_batch_mixed(problems, *, options=None, ctx: Context | None = None, stream=None):
@@ -248,6 +251,82 @@ def solve_stokes_batch_mixed(problems, *, options=None, ctx: Context | None = No
         p.result = r.results()
         out.append(p.result)
     return out
+
+
+class Engine:
+    """Resident solve engine (sf_engine) for continuous batching: :class:`MixedProblem` instances join with
+    :meth:`submit` whenever the arena has room (``None`` when it has not: admission by HBM budget) and
+    leave, written back to their arrays, from the :meth:`step` that sees them converge.  Each instance's
+    result is bit-identical to solving it alone with :func:`solve_stokes_batch_mixed`."""
+
+    def __init__(self, arena_bytes: int, max_instances: int = 1024, *, options=None, ctx: Context | None = None):
+        self._ctx = _ctx(ctx)
+        opt = options if options is not None else mixed_options()
+        h = C.c_void_p()
+        check(lib().sf_engine_create(self._ctx.handle, int(arena_bytes), int(max_instances), C.byref(opt),
+                                     C.byref(h)), "sf_engine_create")
+        self.handle = h.value
+        self._live = {}  # ticket -> MixedProblem; keeps each submitted struct alive at a fixed address
+        self._fin = (C.c_int64 * int(max_instances))()
+
+    @staticmethod
+    def instance_bytes(Nx: int, Ny: int) -> int:
+        b = C.c_int64()
+        check(lib().sf_engine_instance_bytes(int(Nx), int(Ny), C.byref(b)), "sf_engine_instance_bytes")
+        return b.value
+
+    def submit(self, problem: MixedProblem, *, stream=None):
+        """Admit ``problem``; its inputs are read after the work queued on ``stream``.  Returns its ticket,
+        or None when the arena or the instance table is full right now."""
+        t = C.c_int64(-1)
+        st = lib().sf_engine_submit(self.handle, C.byref(problem.c), _stream(stream), C.byref(t))
+        if st == _lib.SF_ERR_BUSY:
+            return None
+        check(st, "sf_engine_submit")
+        self._live[t.value] = problem
+        problem.result = None
+        return t.value
+
+    def step(self, *, stream=None):
+        """One round; returns the problems that finished in it (their arrays written back, ordered on
+        ``stream``; ``problem.result`` set)."""
+        nf, na = C.c_int32(0), C.c_int32(0)
+        # room for every admitted instance: nothing stays pending between calls
+        check(lib().sf_engine_step(self.handle, _stream(stream), self._fin, len(self._fin), C.byref(nf),
+                                   C.byref(na)), "sf_engine_step")
+        done = []
+        for k in range(nf.value):
+            p = self._live.pop(self._fin[k])
+            p.result = p.c.results()
+            done.append(p)
+        return done
+
+    @property
+    def active(self) -> int:
+        return len(self._live)
+
+    def stats(self) -> dict:
+        s = _lib.EngineStats()
+        check(lib().sf_engine_get_stats(self.handle, C.byref(s)), "sf_engine_get_stats")
+        return s.as_dict()
+
+    def close(self):
+        if self.handle:
+            lib().sf_engine_destroy(self.handle)
+            self.handle = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def residual_scale(rho_vy, Nx, Ny, g_y, *, ctx: Context | None = None, stream=None) -> float:

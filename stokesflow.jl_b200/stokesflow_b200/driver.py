@@ -117,7 +117,11 @@ class StokesFlow2D:
         else:
             self.x_m, self.y_m = api.initialize_markers(self.marker_density, self.lx, self.ly, self.dx, self.dy, Nx,
                                                         Ny, self.jitter, self.seed, device=self.device, ctx=self.ctx)
-            self.rho_m, self.mu_m = api.set_initial_marker_properties(self.x_m, self.y_m, self.model, ctx=self.ctx)
+            if hasattr(self.model, "marker_properties"):   # any other material model (workloads.InclusionModel)
+                self.rho_m, self.mu_m = self.model.marker_properties(self.x_m, self.y_m)
+            else:
+                self.rho_m, self.mu_m = api.set_initial_marker_properties(self.x_m, self.y_m, self.model,
+                                                                          ctx=self.ctx)
         self.dt = 0.0
         self.t_tot = 0.0
         self.nt = 0
@@ -213,6 +217,29 @@ class StokesFlow2D:
         rec = dict(nt=self.nt, dt=self.dt, t_tot=self.t_tot, times=t, info=info)
         self.history.append(rec)
         return rec
+
+    # split timestep for a serving loop: the solve runs in a shared engine between the two halves
+    def begin_timestep(self) -> api.MixedProblem:
+        """Deposit (:164-166) and return this timestep's Stokes problem."""
+        self.deposit()
+        return self.mixed_problem()
+
+    def end_timestep(self, result: dict):
+        """After the solve (:171-176): take its dt, advect (:181), rebin if asked, count the timestep."""
+        self.dt = result["dt_out"]
+        self.advect()
+        if self.rebin:
+            self.do_rebin()
+        self.t_tot += self.dt
+        self.nt += 1
+
+    def device_bytes(self) -> int:
+        """Device bytes held by this state (markers and grid arrays)."""
+        ts = [self.x_m, self.y_m, self.rho_m, self.mu_m, self.P, self.Vx, self.Vy, self.rho_vy, self.mu_b, self.mu_p,
+              self.dVxdt, self.dVydt, self.Vx_s, self.Vy_s]
+        ts += [t for t in (self.txx, self.tyy, self.txy, self.divV, self.dtPt, self.Rx, self.Ry, self.dtVx, self.dtVy,
+                           self.val_wt_sum, self.wt_sum) if t is not None]
+        return int(sum(t.numel() * t.element_size() for t in ts))
 
     def h2d_bytes_per_step(self):
         return 4 * 8 * self.n_markers
