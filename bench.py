@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--pt-probe", type=int, default=0, metavar="ITERS",
                     help="kernel probe: run ITERS fused PT iterations of an n x n solve (smooth random fields, no "
                          "markers) and print the kernel time; used for ncu captures")
+    ap.add_argument("--pt32-probe", type=int, default=0, metavar="SWEEPS",
+                    help="kernel probe: one n x n instance through the mixed engine for exactly SWEEPS FP32 sweeps "
+                         "(one fold); prints the sweep time; used for ncu captures of k_pt32")
     ap.add_argument("--form", default="timestep", choices=["timestep", "batch", "serve"],
                     help="timestep: the plain FP64 timestep (default line); batch: many independent solves in one "
                          "engine vs a loop of plain FP64 solves; serve: a Poisson request stream, continuous "
@@ -112,6 +115,32 @@ def pt_probe(a):
     print(json.dumps({"probe": "k_pt_iter", "n": n, "iters": iters, "us_per_iter": round(us, 3),
                       "t_eff_gbs": round(gbs, 1), "frac_of_peak": round(gbs / peak, 4), "peak_source": src,
                       "bytes_per_iter": info["bytes_per_iter"]}), flush=True)
+
+
+def pt32_probe(a):
+    """FP32 sweeps of the mixed engine alone: one n x n instance (smooth random fields), SWEEPS sweeps in one
+    fold, timed by the engine's device clock; the fold's FP64 residual evaluations are a small extra."""
+    import stokesflow_b200 as sf
+    n, sweeps = a.n, a.pt32_probe
+    z = sf.zeros
+    P, Vx, Vy, Vxs, Vys = z(n - 1, n - 1), z(n + 2, n + 1), z(n + 1, n + 2), z(n, n + 1), z(n + 1, n)
+    rho, mub, mup = z(n + 1, n), z(n, n), z(n - 1, n - 1)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for arr in (rho, mub, mup):
+        arr.copy_(1.0 + 0.5 * torch.rand(arr.shape[1], arr.shape[0], device="cuda", dtype=torch.float64,
+                                         generator=g).t())
+    opts = sf.mixed_options(max_sweeps=sweeps, fold_every=sweeps)
+    h = 1.0 / (n - 1)
+    for rep in range(2):   # the first run captures the graph
+        p = sf.MixedProblem(P, Vx, Vy, rho, mub, mup, Vxs, Vys, 9.81, h, h, n, n, 0.0, 0.5, eps=1e-300)
+        r = sf.solve_stokes_batch_mixed([p], options=opts)[0]
+    peak, src = peak_hbm()
+    us = r["batch_ms"] * 1e3 / max(1, r["inner_iters"])
+    pts = (n - 1) * (n - 1)
+    gbs = sf.driver.MIXED_BYTES_PER_POINT * pts / (us * 1e-6) / 1e9
+    print(json.dumps({"probe": "k_pt32", "n": n, "sweeps": r["inner_iters"], "us_per_sweep": round(us, 3),
+                      "gpts_per_s": round(pts / us / 1e3, 2), "t_eff_gbs": round(gbs, 1),
+                      "frac_of_peak": round(gbs / peak, 4), "peak_source": src}), flush=True)
 
 
 def bench_config(a):
@@ -398,13 +427,18 @@ def run_batch_form(a):
                                          rel_tol=a.rtol))
         return probs, arrs
 
-    def fp64_solve(d, s):
+    def fp64_solve(d, s, rtol=a.rtol):
         sp = d["spec"]
         scale = sf.residual_scale(d["rho_vy"], sp.Nx, sp.Ny, 9.81)
-        return sf.solve_stokes_info(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"], None, None,
-                                    None, None, None, None, None, s["dVx"], s["dVy"], None, None, s["Vx_s"],
-                                    s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5, eps=a.rtol * scale,
-                                    iter_max=SOLVE_CAP)
+        try:
+            return sf.solve_stokes_info(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"], None,
+                                        None, None, None, None, None, None, s["dVx"], s["dVy"], None, None, s["Vx_s"],
+                                        s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5,
+                                        eps=rtol * scale, iter_max=SOLVE_CAP)
+        except sf.StokesFlowError as e:
+            if e.status != 5:   # SF_ERR_NONFINITE: the instance diverged; anything else is an error
+                raise
+            return {"converged": 0, "iters": 0, "nonfinite": 1}
 
     # warm-up of both paths on the two smallest instances (graph capture, occupancy queries, scratch growth)
     small = sorted(inst, key=lambda d: d["spec"].points)[:2]
@@ -431,6 +465,19 @@ def run_batch_form(a):
     clk = clocks.stop()
     errs = {f: sorted(_rel_l2(arrs[q][f], fp64_arrs[q][f]) for q in range(k)
                       if res[q]["status"] == 0 and infos[q]["converged"]) for f in ("Vx_pad", "Vy_pad", "P")}
+    # both stopped at rtol are a convergence error away from the discrete solution: measure each against a
+    # tight FP64 solve (relative residual 1e-10) on the smallest timed instances
+    tight = []
+    for q in sorted(range(k), key=lambda q: inst[q]["spec"].points)[:8]:
+        if res[q]["status"] != 0 or not infos[q]["converged"]:
+            continue
+        d = inst[q]
+        t = _state_arrays(sf, d["spec"].Nx, d["spec"].Ny)
+        if not fp64_solve(d, t, rtol=1e-10)["converged"]:
+            continue
+        tight.append({"instance": q, "cells": [d["spec"].Nx - 1, d["spec"].Ny - 1],
+                      **{f"mixed_{f}": _rel_l2(arrs[q][f], t[f]) for f in ("Vx_pad", "Vy_pad", "P")},
+                      **{f"fp64_{f}": _rel_l2(fp64_arrs[q][f], t[f]) for f in ("Vx_pad", "Vy_pad", "P")}})
     pts = [d["spec"].points for d in inst]
     mixed_rate = len(inst) / mixed_s
     fp64_rate = k / fp64_s
@@ -442,10 +489,14 @@ def run_batch_form(a):
             "instances": len(inst), "converged": sum(r["converged"] for r in res),
             "nonfinite": sum(1 for r in res if r["status"] == 5),
             "fp64_converged": sum(int(i["converged"]) for i in infos),
+            "fp64_nonfinite": sum(int(i.get("nonfinite", 0)) for i in infos),
+            "retried": sum(int(r.get("retried", 0)) for r in res),
             "mixed_sweeps_total": int(mixed_sweeps), "fp64_iters_total": int(sum(i["iters"] for i in infos)),
             "fp32_sweep_gpts": round(sum(r["inner_iters"] * pts[q] for q, r in enumerate(res)) / mixed_s / 1e9, 3),
-            "rel_l2_vs_fp64": {f: {"median": v[len(v) // 2] if v else None, "max": v[-1] if v else None}
-                               for f, v in errs.items()},
+            "rel_l2_vs_fp64_same_rtol": {f: {"median": v[len(v) // 2] if v else None, "max": v[-1] if v else None}
+                                         for f, v in errs.items()},
+            "vs_tight_fp64": tight,
+            "nonfinite_instances": [q for q, r in enumerate(res) if r["status"] == 5],
             "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
             "clocks": clk,
             "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {a.batch_cells}, 9-25 "
@@ -534,6 +585,10 @@ def main():
     if a.pt_probe:
         torch.cuda.set_device(local_rank)
         pt_probe(a)
+        return
+    if a.pt32_probe:
+        torch.cuda.set_device(local_rank)
+        pt32_probe(a)
         return
     if a.form != "timestep" and a.impl == "ours":
         if rank == 0:

@@ -185,7 +185,7 @@ typedef struct {
     double eps;                /* absolute stopping tolerance, as solveStokes!'s eps          */
     double rel_tol;            /* if > 0: eps = rel_tol * mean|g_y rho_vy| (relative residual) */
     int32_t use_free_surface_stabilization;
-    int32_t reserved0;
+    int32_t retried;           /* result: 1 if the solve restarted with dtau_local_max (retry_local_max) */
     /* results */
     double dt_out;             /* compute_dt of the final velocities */
     double err;                /* final FP64 residual norm           */
@@ -208,7 +208,10 @@ typedef struct {
                                   (StokesSolver_multixpu.jl:129-130).  The converged solution is the
                                   same either way.  Neither form converges on inclusions much stiffer
                                   than their matrix (100x diverges in FP64 too) (0)                   */
-    int32_t reserved;
+    int32_t retry_local_max;   /* 1: an instance whose residual turns non-finite restarts from its
+                                  inputs with dtau_local_max = 1 (its sweeps keep counting against
+                                  max_sweeps); it converges on mixed soft/stiff layouts where the
+                                  reference's step diverges.  Instances that converge are unaffected (1) */
 } sf_mixed_options;
 
 /* Solves n independent Stokes problems (each as in solveStokes!, with its own

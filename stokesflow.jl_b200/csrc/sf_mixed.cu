@@ -174,27 +174,38 @@ __global__ void __launch_bounds__(NT, 3) k_pt32(const CUtensorMap* __restrict__ 
         RowT* sRvy = reinterpret_cast<RowT*>(tb + 1 * TILE_BYTES);
         RowT* sRx = reinterpret_cast<RowT*>(tb + 2 * TILE_BYTES);
         RowT* sRy = reinterpret_cast<RowT*>(tb + 3 * TILE_BYTES);
-        float* Vx_out = gf(I, in ? G_VXA : G_VXB);
-        float* Vy_out = gf(I, in ? G_VYA : G_VYB);
-        float* P_out = gf(I, in ? G_PA : G_PB);
-        float* Rvx = gf(I, G_RVX);
-        float* Rvy = gf(I, G_RVY);
+        // this tile's corner in the fields; in-tile offsets fit 32 bits
+        const int64_t tbase = i0 + (int64_t)j0 * LD;
+        const int ldi = (int)LD;
+        float* Vx_out = gf(I, in ? G_VXA : G_VXB) + tbase;
+        float* Vy_out = gf(I, in ? G_VYA : G_VYB) + tbase;
+        float* P_out = gf(I, in ? G_PA : G_PB) + tbase;
+        float* Rvx = gf(I, G_RVX) + tbase;
+        float* Rvy = gf(I, G_RVY) + tbase;
+        const float c_pt = I.c_ptscf, dampX = I.dampXf, dampY = I.dampYf, g_dt = I.g_dtf;
+        // pseudo-time step c_vsc / mu_av = (2 c_vsc) / (mu_0 + mu_1) (the reference's average, :129-130), or
+        // c_vsc / (largest viscosity of the node's stencil); the FP32 sweeps only drive the correction, so the
+        // fast division is enough
+        const float c_vsc = I.c_vscf, c_vsc2 = 2.0f * I.c_vscf;
+        const bool dmax = I.dtau_max != 0;
+        // interior tiles: every point of the tile and its halo is inside, no boundary node among them
+        const bool interior = i0 > 0 && j0 > 0 && i0 + BX + 2 < Nx && j0 + BY + 2 < Ny;
 
         // ---- stage 1: P and tau of the correction on tile + 1 halo ----
         for (int idx = tid; idx < W1 * H1; idx += NT) {
             const int b = idx / W1, a = idx - b * W1;
             const int i = i0 + a, j = j0 + b;
-            if (i < Nx - 1 && j < Ny - 1) {
+            if (interior || (i < Nx - 1 && j < Ny - 1)) {
                 float dVx_dx = (sVx[b + 1][a + 1] - sVx[b + 1][a]) * _dx;
                 float dVy_dy = (sVy[b + 1][a + 1] - sVy[b][a + 1]) * _dy;
                 float div_d = dVx_dx + dVy_dy;
                 float div_full = div_d + sRdiv[b][a];          // divV of V_k + dV
                 float mu = sMup[b][a];
-                sPn[b][a] = sPo[b][a] - I.c_ptscf * mu * div_full;
+                sPn[b][a] = sPo[b][a] - c_pt * mu * div_full;
                 sTxx[b][a] = 2.0f * mu * (dVx_dx - (1.0f / 3.0f) * div_d);
                 sTyy[b][a] = 2.0f * mu * (dVy_dy - (1.0f / 3.0f) * div_d);
             }
-            if (i < Nx && j < Ny) {
+            if (interior || (i < Nx && j < Ny)) {
                 float dVx_dy = (sVx[b + 1][a] - sVx[b][a]) * _dy;
                 float dVy_dx = (sVy[b][a + 1] - sVy[b][a]) * _dx;
                 sTxy[b][a] = sMub[b][a] * (dVx_dy + dVy_dx);
@@ -202,56 +213,72 @@ __global__ void __launch_bounds__(NT, 3) k_pt32(const CUtensorMap* __restrict__ 
         }
         __syncthreads();
         // ---- stage 2: damped rates and velocity update of the correction ----
+        auto rate_x = [&](int a, int b, int o) {
+            float Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy -
+                       (sPn[b][a + 1] - sPn[b][a]) * _dx + sRx[b][a];
+            float dv = dampX * sRvx[b][a] + Rx;
+            Rvx[o] = dv;
+            float dtau = dmax ? __fdividef(c_vsc, fmaxf(fmaxf(sMup[b][a], sMup[b][a + 1]),
+                                                       fmaxf(sMub[b][a + 1], sMub[b + 1][a + 1])))
+                              : __fdividef(c_vsc2, sMup[b][a] + sMup[b][a + 1]);
+            return sVx[b + 1][a + 1] + dtau * dv;
+        };
+        auto rate_y = [&](int a, int b, int o) {
+            float av = 0.25f * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
+            float dxr = sRho[b + 1][a + 2] - sRho[b + 1][a];
+            float dyr = sRho[b + 2][a + 1] - sRho[b][a + 1];
+            float Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx -
+                       (sPn[b + 1][a] - sPn[b][a]) * _dy -
+                       g_dt * (av * dxr * 0.5f * _dx + sVy[b + 1][a + 1] * dyr * 0.5f * _dy) + sRy[b][a];
+            float dv = dampY * sRvy[b][a] + Ry;
+            Rvy[o] = dv;
+            float dtau = dmax ? __fdividef(c_vsc, fmaxf(fmaxf(sMup[b][a], sMup[b + 1][a]),
+                                                       fmaxf(sMub[b + 1][a], sMub[b + 1][a + 1])))
+                              : __fdividef(c_vsc2, sMup[b][a] + sMup[b + 1][a]);
+            return sVy[b + 1][a + 1] + dtau * dv;
+        };
+        if (interior) {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int a = tx, b = ty + r * TY;
-            const int i = i0 + a, j = j0 + b;
-            if (i >= Nx - 1 || j >= Ny - 1) continue;
-            const int64_t o = i + (int64_t)j * LD;
-            P_out[o] = sPn[b][a];
-            if (i < Nx - 2) {
-                float Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy -
-                           (sPn[b][a + 1] - sPn[b][a]) * _dx + sRx[b][a];
-                float dv = I.dampXf * sRvx[b][a] + Rx;
-                Rvx[o] = dv;
-                // pseudo-time step: the reference's average of the two pressure-cell viscosities
-                // (:129), or the largest viscosity of the node's stencil (stable at high contrast)
-                float mux = I.dtau_max ? fmaxf(fmaxf(sMup[b][a], sMup[b][a + 1]), fmaxf(sMub[b][a + 1], sMub[b + 1][a + 1]))
-                                       : (sMup[b][a] + sMup[b][a + 1]) * 0.5f;
-                float dtau = I.c_vscf / mux;
-                float vn = sVx[b + 1][a + 1] + dtau * dv;
-                Vx_out[o + 1 + LD] = vn;
-                if (j == 0) Vx_out[o + 1] = vn;
-                if (j == Ny - 2) Vx_out[o + 1 + 2 * LD] = vn;
+            for (int r = 0; r < RPT; ++r) {
+                const int a = tx, b = ty + r * TY;
+                const int o = a + b * ldi;
+                P_out[o] = sPn[b][a];
+                Vx_out[o + 1 + ldi] = rate_x(a, b, o);
+                Vy_out[o + 1 + ldi] = rate_y(a, b, o);
             }
-            if (j < Ny - 2) {
-                float av = 0.25f * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
-                float dxr = sRho[b + 1][a + 2] - sRho[b + 1][a];
-                float dyr = sRho[b + 2][a + 1] - sRho[b][a + 1];
-                float Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx -
-                           (sPn[b + 1][a] - sPn[b][a]) * _dy -
-                           I.g_dtf * (av * dxr * 0.5f * _dx + sVy[b + 1][a + 1] * dyr * 0.5f * _dy) + sRy[b][a];
-                float dv = I.dampYf * sRvy[b][a] + Ry;
-                Rvy[o] = dv;
-                float muy = I.dtau_max ? fmaxf(fmaxf(sMup[b][a], sMup[b + 1][a]), fmaxf(sMub[b + 1][a], sMub[b + 1][a + 1]))
-                                       : (sMup[b][a] + sMup[b + 1][a]) * 0.5f;
-                float dtau = I.c_vscf / muy;
-                float vn = sVy[b + 1][a + 1] + dtau * dv;
-                Vy_out[o + 1 + LD] = vn;
-                if (i == 0) Vy_out[o + LD] = vn;
-                if (i == Nx - 2) Vy_out[o + 2 + LD] = vn;
-            }
-            if (i == 0 || i == Nx - 2) {
-                int ic = (i == 0) ? 0 : Nx - 1;
-                Vx_out[ic + (int64_t)(j + 1) * LD] = 0.f;
-                if (j == 0) Vx_out[ic] = 0.f;
-                if (j == Ny - 2) Vx_out[ic + (int64_t)Ny * LD] = 0.f;
-            }
-            if (j == 0 || j == Ny - 2) {
-                int64_t jr = (j == 0) ? 0 : (int64_t)(Ny - 1) * LD;
-                Vy_out[(i + 1) + jr] = 0.f;
-                if (i == 0) Vy_out[jr] = 0.f;
-                if (i == Nx - 2) Vy_out[Nx + jr] = 0.f;
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int a = tx, b = ty + r * TY;
+                const int i = i0 + a, j = j0 + b;
+                if (i >= Nx - 1 || j >= Ny - 1) continue;
+                const int o = a + b * ldi;
+                P_out[o] = sPn[b][a];
+                if (i < Nx - 2) {
+                    float vn = rate_x(a, b, o);
+                    Vx_out[o + 1 + ldi] = vn;
+                    if (j == 0) Vx_out[o + 1] = vn;
+                    if (j == Ny - 2) Vx_out[o + 1 + 2 * ldi] = vn;
+                }
+                if (j < Ny - 2) {
+                    float vn = rate_y(a, b, o);
+                    Vy_out[o + 1 + ldi] = vn;
+                    if (i == 0) Vy_out[o + ldi] = vn;
+                    if (i == Nx - 2) Vy_out[o + 2 + ldi] = vn;
+                }
+                // free-slip rows / columns: relative to the tile corner (i0, j0)
+                if (i == 0 || i == Nx - 2) {
+                    int ac = (i == 0) ? -i0 : Nx - 1 - i0;
+                    Vx_out[ac + (b + 1) * ldi] = 0.f;
+                    if (j == 0) Vx_out[ac - j0 * ldi] = 0.f;
+                    if (j == Ny - 2) Vx_out[ac + (Ny - j0) * ldi] = 0.f;
+                }
+                if (j == 0 || j == Ny - 2) {
+                    int br = (j == 0) ? -j0 : Ny - 1 - j0;
+                    Vy_out[(a + 1) + br * ldi] = 0.f;
+                    if (i == 0) Vy_out[-i0 + br * ldi] = 0.f;
+                    if (i == Nx - 2) Vy_out[Nx - i0 + br * ldi] = 0.f;
+                }
             }
         }
         __syncthreads();  // stage s and the stage-1 arrays are free again
@@ -607,6 +634,7 @@ static sf_mixed_options normalized(const sf_mixed_options* o) {
         r.fold_every = 400;
         r.use_graphs = 1;
         r.dtau_local_max = 0;
+        r.retry_local_max = 1;
     }
     if (r.fold_every < 2) r.fold_every = 2;
     r.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
@@ -802,7 +830,7 @@ int launch_sweeps(sf_engine* e) {
 }
 
 // packs the caller's arrays of slot q into the arena and fills its device record and tensor maps
-int admit(sf_engine* e, int q, sf_batch_instance& u) {
+int admit(sf_engine* e, int q, sf_batch_instance& u, int dtau_max) {
     sf_ctx* ctx = e->ctx;
     cudaStream_t s = e->s;
     Slot& h = e->slots[q];
@@ -829,7 +857,7 @@ int admit(sf_engine* e, int q, sf_batch_instance& u) {
     I.g_y = u.g_y;
     I.maxdisp = u.maxdisp;
     I.use_stab = u.use_free_surface_stabilization ? 1 : 0;
-    I.dtau_max = e->opt.dtau_local_max ? 1 : 0;
+    I.dtau_max = dtau_max;
     I.dt_in = I.use_stab ? u.dt : 0.0;
     I.dt = I.dt_in;
     I._dxf = (float)I._dx;
@@ -933,7 +961,8 @@ int engine_submit(sf_engine* e, sf_batch_instance* u, cudaStream_t caller, int64
     // the inputs are ready once the work queued on the caller's stream is done
     SF_CUDA(cudaEventRecord(e->ev_in, caller));
     SF_CUDA(cudaStreamWaitEvent(e->s, e->ev_in, 0));
-    if ((rc = admit(e, q, *u))) {
+    u->retried = 0;
+    if ((rc = admit(e, q, *u, e->opt.dtau_local_max ? 1 : 0))) {
         e->alloc.release(off, bytes);
         e->free_slots.push_back(q);
         return rc;
@@ -989,6 +1018,13 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
         ++h.outer;
         h.swept = false;
         const bool bad = !(h.err == h.err) || std::isinf(h.err);
+        if (bad && e->opt.retry_local_max && !h.d.dtau_max && h.inner_total < e->opt.max_sweeps) {
+            // restart from the caller's inputs (untouched until write-back) with the stencil-maximum
+            // pseudo-time step; it re-enters with the next round's residual, its sweeps keep counting
+            if ((rc = admit(e, q, *h.user, 1))) return rc;
+            h.user->retried = 1;
+            continue;
+        }
         if (bad || h.err <= h.eps || h.inner_total >= e->opt.max_sweeps) {
             if ((rc = write_back(e, q, e->h_out[3 * k + 2]))) return rc;
             h.active = false;

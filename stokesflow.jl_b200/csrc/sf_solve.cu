@@ -200,6 +200,8 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         RowD* sDtx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 2 * DV_BYTES);  // dtauVx of :129
         RowD* sDty = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 3 * DV_BYTES);  // dtauVy of :130
         const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
+        // interior tiles: every point of the tile and its halo is inside, no boundary node among them
+        const bool interior = i0 > 0 && j0 > 0 && i0 + BX + 2 < Nx && j0 + BY + 2 < Ny;
 
         // ---- stage 1: compute_P_tau! (:140-169) on tile + 1 halo ----
         // the (BX+1) x (BY+1) points are spread evenly over all threads, row by row
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
             {
                 const int b = idx / W1, a = idx - b * W1;
                 const int i = i0 + a, j = j0 + b;
-                if (i < Nx - 1 && j < Ny - 1) {
+                if (interior || (i < Nx - 1 && j < Ny - 1)) {
                     double vx1 = sVx[b + 1][a], vx2 = sVx[b + 1][a + 1];
                     double vy1 = sVy[b][a + 1], vy2 = sVy[b + 1][a + 1];
                     double dVx_dx = (vx2 - vx1) * _dx;
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
                         p.tyy[o] = tyy;
                     }
                 }
-                if (i < Nx && j < Ny) {
+                if (interior || (i < Nx && j < Ny)) {
                     double vx0 = sVx[b][a], vx1 = sVx[b + 1][a];
                     double vy0 = sVy[b][a], vy1 = sVy[b][a + 1];
                     double dVx_dy = (vx1 - vx0) * _dy;
@@ -243,51 +245,77 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         __syncthreads();
 
         // ---- stage 2: compute_dV! (:209-219), compute_V! (:226-234), BCs (:53-56) ----
+        // offsets are taken from the tile corner (i0, j0); in-tile offsets fit 32 bits
+        const int64_t tbase = i0 + (int64_t)j0 * LD;
+        const int ldi = (int)LD;
+        double* const P_t = p.P_out + tbase;
+        double* const dVx_t = p.dVx + tbase;
+        double* const dVy_t = p.dVy + tbase;
+        double* const Vx_t = p.Vx_out + tbase;
+        double* const Vy_t = p.Vy_out + tbase;
+        auto new_vx = [&](int a, int b, int o) {
+            // compute_ResX (:176-182)
+            double Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy
+                        - (sPn[b][a + 1] - sPn[b][a]) * _dx;
+            double dv = p.dampX * sDvx[b][a] + Rx;
+            dVx_t[o] = dv;
+            return sVx[b + 1][a + 1] + sDtx[b][a] * dv;
+        };
+        auto new_vy = [&](int a, int b, int o) {
+            // compute_ResY (:189-202)
+            double av_inn_y_Vx = 0.25 * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
+            double d_xi_2_rho = sRho[b + 1][a + 2] - sRho[b + 1][a];
+            double d_yi_2_rho = sRho[b + 2][a + 1] - sRho[b][a + 1];
+            double Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx
+                        - (sPn[b + 1][a] - sPn[b][a]) * _dy
+                        + p.g_y * (sRho[b + 1][a + 1] - dt * (av_inn_y_Vx * d_xi_2_rho * 0.5 * _dx
+                                                               + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
+            double dv = p.dampY * sDvy[b][a] + Ry;
+            dVy_t[o] = dv;
+            return sVy[b + 1][a + 1] + sDty[b][a] * dv;
+        };
+        if (interior) {
 #pragma unroll
-        for (int r = 0; r < RPT; ++r) {
-            const int a = tx, b = ty + r * TY;
-            const int i = i0 + a, j = j0 + b;
-            if (i >= Nx - 1 || j >= Ny - 1) continue;
-            p.P_out[i + (int64_t)j * LD] = sPn[b][a];
-            if (i < Nx - 2) {
-                // compute_ResX (:176-182)
-                double Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy
-                            - (sPn[b][a + 1] - sPn[b][a]) * _dx;
-                double dv = p.dampX * sDvx[b][a] + Rx;
-                p.dVx[i + (int64_t)j * LD] = dv;
-                double vn = sVx[b + 1][a + 1] + sDtx[b][a] * dv;
-                p.Vx_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
-                if (j == 0) p.Vx_out[(i + 1)] = vn;                                   // bc_y_noflux!
-                if (j == Ny - 2) p.Vx_out[(i + 1) + (int64_t)Ny * LD] = vn;
+            for (int r = 0; r < RPT; ++r) {
+                const int a = tx, b = ty + r * TY;
+                const int o = a + b * ldi;
+                P_t[o] = sPn[b][a];
+                Vx_t[o + 1 + ldi] = new_vx(a, b, o);
+                Vy_t[o + 1 + ldi] = new_vy(a, b, o);
             }
-            if (j < Ny - 2) {
-                // compute_ResY (:189-202)
-                double av_inn_y_Vx = 0.25 * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
-                double d_xi_2_rho = sRho[b + 1][a + 2] - sRho[b + 1][a];
-                double d_yi_2_rho = sRho[b + 2][a + 1] - sRho[b][a + 1];
-                double Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx
-                            - (sPn[b + 1][a] - sPn[b][a]) * _dy
-                            + p.g_y * (sRho[b + 1][a + 1] - dt * (av_inn_y_Vx * d_xi_2_rho * 0.5 * _dx
-                                                                   + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
-                double dv = p.dampY * sDvy[b][a] + Ry;
-                p.dVy[i + (int64_t)j * LD] = dv;
-                double vn = sVy[b + 1][a + 1] + sDty[b][a] * dv;
-                p.Vy_out[(i + 1) + (int64_t)(j + 1) * LD] = vn;
-                if (i == 0) p.Vy_out[(int64_t)(j + 1) * LD] = vn;                     // bc_x_noflux!
-                if (i == Nx - 2) p.Vy_out[Nx + (int64_t)(j + 1) * LD] = vn;
-            }
-            // constant free-slip entries: bc_x_zero!(Vx) and bc_y_zero!(Vy), corners included
-            if (i == 0 || i == Nx - 2) {
-                int ic = (i == 0) ? 0 : Nx - 1;
-                p.Vx_out[ic + (int64_t)(j + 1) * LD] = 0.0;
-                if (j == 0) p.Vx_out[ic] = 0.0;
-                if (j == Ny - 2) p.Vx_out[ic + (int64_t)Ny * LD] = 0.0;
-            }
-            if (j == 0 || j == Ny - 2) {
-                int64_t jr = (j == 0) ? 0 : (int64_t)(Ny - 1) * LD;
-                p.Vy_out[(i + 1) + jr] = 0.0;
-                if (i == 0) p.Vy_out[jr] = 0.0;
-                if (i == Nx - 2) p.Vy_out[Nx + jr] = 0.0;
+        } else {
+#pragma unroll
+            for (int r = 0; r < RPT; ++r) {
+                const int a = tx, b = ty + r * TY;
+                const int i = i0 + a, j = j0 + b;
+                if (i >= Nx - 1 || j >= Ny - 1) continue;
+                const int o = a + b * ldi;
+                P_t[o] = sPn[b][a];
+                if (i < Nx - 2) {
+                    double vn = new_vx(a, b, o);
+                    Vx_t[o + 1 + ldi] = vn;
+                    if (j == 0) Vx_t[o + 1] = vn;                                       // bc_y_noflux!
+                    if (j == Ny - 2) Vx_t[o + 1 + 2 * ldi] = vn;
+                }
+                if (j < Ny - 2) {
+                    double vn = new_vy(a, b, o);
+                    Vy_t[o + 1 + ldi] = vn;
+                    if (i == 0) Vy_t[o + ldi] = vn;                                     // bc_x_noflux!
+                    if (i == Nx - 2) Vy_t[o + 2 + ldi] = vn;
+                }
+                // constant free-slip entries: bc_x_zero!(Vx) and bc_y_zero!(Vy), corners included
+                if (i == 0 || i == Nx - 2) {
+                    int ac = (i == 0) ? -i0 : Nx - 1 - i0;
+                    Vx_t[ac + (b + 1) * ldi] = 0.0;
+                    if (j == 0) Vx_t[ac - j0 * ldi] = 0.0;
+                    if (j == Ny - 2) Vx_t[ac + (Ny - j0) * ldi] = 0.0;
+                }
+                if (j == 0 || j == Ny - 2) {
+                    int br = (j == 0) ? -j0 : Ny - 1 - j0;
+                    Vy_t[(a + 1) + br * ldi] = 0.0;
+                    if (i == 0) Vy_t[-i0 + br * ldi] = 0.0;
+                    if (i == Nx - 2) Vy_t[Nx - i0 + br * ldi] = 0.0;
+                }
             }
         }
         __syncthreads();  // stage s and the stage-1 arrays are free again

@@ -57,11 +57,12 @@ class BatchInstance(C.Structure):
     _fields_ = [("P", _vp), ("Vx_pad", _vp), ("Vy_pad", _vp), ("rho_vy", _vp), ("mu_b", _vp), ("mu_p", _vp),
                 ("Vx_s", _vp), ("Vy_s", _vp), ("Nx", _i64), ("Ny", _i64), ("g_y", _d), ("dx", _d), ("dy", _d),
                 ("dt", _d), ("maxdisp", _d), ("eps", _d), ("rel_tol", _d),
-                ("use_free_surface_stabilization", _i32), ("reserved0", _i32), ("dt_out", _d), ("err", _d),
+                ("use_free_surface_stabilization", _i32), ("retried", _i32), ("dt_out", _d), ("err", _d),
                 ("eps_used", _d), ("inner_iters", _i64), ("outer_iters", _i64), ("converged", _i32),
                 ("status", _i32), ("batch_ms", _d)]
 
-    RESULTS = ("dt_out", "err", "eps_used", "inner_iters", "outer_iters", "converged", "status", "batch_ms")
+    RESULTS = ("dt_out", "err", "eps_used", "inner_iters", "outer_iters", "converged", "status", "batch_ms",
+               "retried")
 
     def results(self):
         return {k: getattr(self, k) for k in self.RESULTS}
@@ -70,7 +71,7 @@ class BatchInstance(C.Structure):
 class MixedOptions(C.Structure):
     """sf_mixed_options."""
     _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32), ("dtau_local_max", _i32),
-                ("reserved", _i32)]
+                ("retry_local_max", _i32)]
 
 
 class EngineStats(C.Structure):

@@ -230,11 +230,14 @@ class MixedProblem:
         self.result = None
 
 
-def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True, dtau_local_max=False):
+def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True, dtau_local_max=False,
+                  retry_local_max=True):
     """Options of the mixed-precision / batched solver (sf_mixed_options).  dtau_local_max: pseudo-time
     steps from the stencil's largest viscosity instead of the reference's average (faster on soft
-    inclusions); the converged solution is the same."""
-    return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)), int(bool(dtau_local_max)), 0)
+    inclusions); the converged solution is the same.  retry_local_max: an instance that diverges restarts
+    from its inputs with the stencil-maximum step."""
+    return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)), int(bool(dtau_local_max)),
+                             int(bool(retry_local_max)))
 
 
 def solve_stokes_batch_mixed(problems, *, options=None, ctx: Context | None = None, stream=None):
