@@ -70,10 +70,15 @@ def parse():
     ap.add_argument("--pt32-probe", type=int, default=0, metavar="SWEEPS",
                     help="kernel probe: one n x n instance through the mixed engine for exactly SWEEPS FP32 sweeps "
                          "(one fold); prints the sweep time; used for ncu captures of k_pt32")
-    ap.add_argument("--form", default="timestep", choices=["timestep", "batch", "serve"],
-                    help="timestep: the plain FP64 timestep (default line); batch: many independent solves in one "
+    ap.add_argument("--form", default="timestep", choices=["timestep", "precision", "batch", "serve"],
+                    help="timestep: the plain FP64 timestep (default line); precision: the same timesteps with FP32 "
+                         "sweeps + FP64 correction beside the plain path; batch: many independent solves in one "
                          "engine vs a loop of plain FP64 solves; serve: a Poisson request stream, continuous "
                          "batching vs plain FP64 serving")
+    ap.add_argument("--precision-cases", type=int, default=2, help="precision form: plume contrasts drawn from seed")
+    ap.add_argument("--precision-contrast", default="0,2",
+                    help="precision form: log10 range of matrix/plume viscosity, log-uniform (soft plume)")
+    ap.add_argument("--precision-steps", type=int, default=3, help="precision form: timesteps per case")
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--batch-cells", default="127,1023", help="cells per side, log-uniform range")
     ap.add_argument("--mu-log10", default="-2,1", help="inclusion viscosity range (log10), log-uniform")
@@ -404,6 +409,61 @@ def _rel_l2(a, b):
     return d / n if n > 0 else d
 
 
+def run_precision_form(a):
+    """Precision form: the plume timesteps of the default workload (n x n grid points, markers per cell as
+    given) with the plume viscosity drawn from seed (matrix/plume contrast log-uniform over
+    10**precision_contrast), each timestep solved twice from the same deposited state: plain FP64 and FP32
+    sweeps + FP64 defect correction, both to relative residual rtol.  Reported per case: solve time of each
+    and the relative L2 distance of V and P between them after every timestep (both carry their own state
+    forward; markers advect with their own velocities)."""
+    import numpy as np
+    import stokesflow_b200 as sf
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(a.seed)
+    lo, hi = _pair(a.precision_contrast)
+    md = sf.driver.marker_density_for(a.markers_per_cell)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+    clocks = ClockSampler(0)
+    clocks.start()
+    cases = []
+    for c in range(a.precision_cases):
+        contrast = float(10.0 ** rng.uniform(lo, hi))
+        model = sf.plume_model_unit_square()
+        model.mu_air = a.mu_air
+        model.mu_plume = model.mu_matrix / contrast
+        states = {s: sf.StokesFlow2D(a.n, a.n, 1.0, 1.0, model, marker_density=md, stokes_rtol=a.rtol, jitter=0.5,
+                                     seed=0, iter_max=SOLVE_CAP, keep_work_arrays=False, solver=s, mixed_opts=opts)
+                  for s in ("fp64", "mixed")}
+        steps = []
+        for k in range(a.precision_steps):
+            rec = {s: st.step() for s, st in states.items()}
+            f, m = states["fp64"], states["mixed"]
+            steps.append({"fp64_solve_ms": round(rec["fp64"]["times"].solve_ms, 2),
+                          "mixed_solve_ms": round(rec["mixed"]["times"].solve_ms, 2),
+                          "fp64_iters": int(rec["fp64"]["info"]["iters"]),
+                          "mixed_sweeps": int(rec["mixed"]["info"]["inner_iters"]),
+                          "rel_l2_Vx": _rel_l2(m.Vx, f.Vx), "rel_l2_Vy": _rel_l2(m.Vy, f.Vy),
+                          "rel_l2_P": _rel_l2(m.P, f.P), "rel_l2_markers_x": _rel_l2(m.x_m, f.x_m)})
+        fs = sum(s["fp64_solve_ms"] for s in steps)
+        ms = sum(s["mixed_solve_ms"] for s in steps)
+        cases.append({"contrast": contrast, "mu_plume": model.mu_plume, "fp64_solve_ms_total": round(fs, 1),
+                      "mixed_solve_ms_total": round(ms, 1), "solve_speedup": round(fs / ms, 3), "steps": steps})
+        del states
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    worst = {k: max(s[k] for cs in cases for s in cs["steps"]) for k in ("rel_l2_Vx", "rel_l2_Vy", "rel_l2_P")}
+    fs = sum(cs["fp64_solve_ms_total"] for cs in cases)
+    ms = sum(cs["mixed_solve_ms_total"] for cs in cases)
+    return {"form": "precision", "metric": f"solve time and rel L2 vs plain FP64, relative residual {a.rtol:g}",
+            "unit": "ms / rel L2", "solve_speedup": round(fs / ms, 3), "worst_rel_l2": worst, "cases": cases,
+            "dtype": "f32 sweeps + f64 correction / f64", "data": "synthetic (seeded markers and contrasts)",
+            "clocks": clk,
+            "config": {"workload": f"plume, {a.n - 1}x{a.n - 1} cells, {a.markers_per_cell} markers/cell, matrix/"
+                                   f"plume viscosity contrast log-uniform 10**[{a.precision_contrast}], "
+                                   f"{a.precision_steps} warm-started timesteps per case, air mu {a.mu_air:g}",
+                       "fold_every": a.fold_every, "seed": a.seed}}
+
+
 def run_batch_form(a):
     """Batching form: N independent problems (seeded random grids and inclusion layouts) solved to relative
     residual rtol in ONE engine run (FP32 sweeps + FP64 defect correction, one launch per sweep for all
@@ -592,8 +652,8 @@ def main():
         return
     if a.form != "timestep" and a.impl == "ours":
         if rank == 0:
-            out = run_batch_form(a) if a.form == "batch" else run_serve_form(a)
-            print(json.dumps(out), flush=True)
+            run = {"precision": run_precision_form, "batch": run_batch_form, "serve": run_serve_form}[a.form]
+            print(json.dumps(run(a)), flush=True)
         return
     if a.impl == "reference":
         out = run_reference(a, rank)
