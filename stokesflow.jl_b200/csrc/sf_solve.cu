@@ -93,8 +93,10 @@ struct PTParams {
 // overlap the arithmetic without needing high occupancy.  A stage holds the
 // old Vx, Vy, rho_vy, P, mu_p, mu_b boxes (tile + 2 halo; the TMA zero-fills
 // beyond the arrays) and the dVx, dVy boxes (tile only).
+// 32 x 8 tiles: 60 KB of shared memory per CTA, 3 CTAs per SM (32 x 16 allowed 2; same speed at 2048^2,
+// 10% faster at 4096^2)
 #ifndef SF_PT_BY
-#define SF_PT_BY 16
+#define SF_PT_BY 8
 #endif
 #ifndef SF_PT_TY
 #define SF_PT_TY 8
