@@ -46,7 +46,14 @@
 namespace sf {
 namespace mx {
 
-constexpr int BX = 32, BY = 16, TY = 8, RPT = BY / TY, NT = BX * TY;
+#ifndef SF_PT32_BY
+#define SF_PT32_BY 16        // tile rows (a multiple of the 8 thread rows)
+#endif
+#ifndef SF_PT32_MINB
+#define SF_PT32_MINB 3       // CTAs per SM the register budget is sized for
+#endif
+constexpr int BX = 32, BY = SF_PT32_BY, TY = 8, RPT = BY / TY, NT = BX * TY;
+static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
 constexpr int TW = 36, TH = BY + 2;   // staged halo box; TW*4 bytes is a multiple of 16
 constexpr int W1 = BX + 1, H1 = BY + 1;
 constexpr int r128(int b) { return (b + 127) / 128 * 128; }
@@ -88,7 +95,7 @@ __device__ __forceinline__ double* gd(const Inst& I, int k) { return I.f64 + (in
 // ---------------------------------------------------------------------------
 // FP32 PT sweep over a tile work list (tiles: {instance, tile index})
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT, 3) k_pt32(const CUtensorMap* __restrict__ maps, const Inst* __restrict__ insts,
+__global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __restrict__ maps, const Inst* __restrict__ insts,
                                                const int2* __restrict__ tiles, const int* __restrict__ ntiles_ptr,
                                                int launch_parity, int* __restrict__ err_flag) {
     extern __shared__ __align__(128) unsigned char smem[];
