@@ -143,24 +143,27 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
             if (t + k * G < ntiles) issue(t + k * G, k);
     uint32_t phase = 0;
     int s = 0;
+    // a copy never completed: flag it, give every copy still in flight a bounded chance to land (the issuing
+    // thread knows their phases), leave together
+    auto give_up = [&]() {
+        if (tid == 0) {
+            atomicExch(err_flag, 1);
+            for (int k = 0; k < NST; ++k) {
+                if (t + k * G >= ntiles) break;
+                const int sk = (s + k) % NST;
+                const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
+                mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
+            }
+        }
+        __syncthreads();
+    };
     for (; t < ntiles; t += G) {
         const int tn = t + (NST - 1) * G;
         if (tid == 0 && tn < ntiles) issue(tn, (s + NST - 1) % NST);
+        // the timeout vote rides on the stage-1 barrier below: stage 1 writes shared memory only, so a thread
+        // whose copy did not land computes garbage there and nothing else before everyone leaves
         const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
         phase ^= 1u << s;
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                atomicExch(err_flag, 1);
-                for (int k = 0; k < NST; ++k) {
-                    if (t + k * G >= ntiles) break;
-                    const int sk = (s + k) % NST;
-                    const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
-                    mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
-                }
-            }
-            __syncthreads();
-            return;
-        }
         const int2 td = tiles[t];
         const Inst& I = insts[td.x];
         const int Nx = I.Nx, Ny = I.Ny;
@@ -199,8 +202,7 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         const bool interior = i0 > 0 && j0 > 0 && i0 + BX + 2 < Nx && j0 + BY + 2 < Ny;
 
         // ---- stage 1: P and tau of the correction on tile + 1 halo ----
-        for (int idx = tid; idx < W1 * H1; idx += NT) {
-            const int b = idx / W1, a = idx - b * W1;
+        auto stage1 = [&](int a, int b) {
             const int i = i0 + a, j = j0 + b;
             if (interior || (i < Nx - 1 && j < Ny - 1)) {
                 float dVx_dx = (sVx[b + 1][a + 1] - sVx[b + 1][a]) * _dx;
@@ -217,8 +219,16 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
                 float dVy_dx = (sVy[b][a + 1] - sVy[b][a]) * _dx;
                 sTxy[b][a] = sMub[b][a] * (dVx_dy + dVy_dx);
             }
+        };
+        // the (BX+1) x (BY+1) points spread evenly over all threads, row by row
+        for (int idx = tid; idx < W1 * H1; idx += NT) {
+            const int b = idx / W1, a = idx - b * W1;
+            stage1(a, b);
         }
-        __syncthreads();
+        if (__syncthreads_or(!ok)) {
+            give_up();
+            return;
+        }
         // ---- stage 2: damped rates and velocity update of the correction ----
         auto rate_x = [&](int a, int b, int o) {
             float Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy -

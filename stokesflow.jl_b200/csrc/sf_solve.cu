@@ -174,22 +174,11 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         // refill the stage freed by the previous tile with the tile NST-1 ahead
         const int tn = t + (NST - 1) * G;
         if (tid == 0 && tn < ntiles) issue(tn, (s + NST - 1) % NST);
+        // the timeout vote rides on the stage-1 barrier below: stage 1 writes shared memory only (and, in the
+        // check variant, tau/divV, which a failed solve discards), so a thread whose copy did not land
+        // computes garbage and nothing else before everyone leaves
         const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
         phase ^= 1u << s;
-        if (__syncthreads_or(!ok)) {
-            // a copy never completed: flag it, give every copy still in flight a bounded chance to land, leave
-            if (tid == 0) {
-                atomicExch(p.err_flag, 1);
-                for (int k = 0; k < NST; ++k) {
-                    if (t + k * G >= ntiles) break;
-                    const int sk = (s + k) % NST;
-                    const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
-                    mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
-                }
-            }
-            __syncthreads();
-            return;
-        }
         unsigned char* st = smem + s * STAGE_BYTES;
         Row2* sVx = reinterpret_cast<Row2*>(st + S_VX * ARR_BYTES);
         Row2* sVy = reinterpret_cast<Row2*>(st + S_VY * ARR_BYTES);
@@ -244,7 +233,20 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
                 }
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(!ok)) {
+            // a copy never completed: flag it, give every copy still in flight a bounded chance to land, leave
+            if (tid == 0) {
+                atomicExch(p.err_flag, 1);
+                for (int k = 0; k < NST; ++k) {
+                    if (t + k * G >= ntiles) break;
+                    const int sk = (s + k) % NST;
+                    const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
+                    mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
+                }
+            }
+            __syncthreads();
+            return;
+        }
 
         // ---- stage 2: compute_dV! (:209-219), compute_V! (:226-234), BCs (:53-56) ----
         // offsets are taken from the tile corner (i0, j0); in-tile offsets fit 32 bits
