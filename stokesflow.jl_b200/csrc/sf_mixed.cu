@@ -50,7 +50,7 @@ namespace mx {
 #define SF_PT32_BY 16        // tile rows (a multiple of the 8 thread rows)
 #endif
 #ifndef SF_PT32_MINB
-#define SF_PT32_MINB 3       // CTAs per SM the register budget is sized for
+#define SF_PT32_MINB 4       // CTAs per SM the register budget is sized for (56 KB of shared memory each)
 #endif
 constexpr int BX = 32, BY = SF_PT32_BY, TY = 8, RPT = BY / TY, NT = BX * TY;
 static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
@@ -65,7 +65,7 @@ constexpr int STAGE_BYTES = NHALO * HALO_BYTES + NTILE * TILE_BYTES;
 constexpr uint32_t STAGE_TX = NHALO * TH * TW * 4 + NTILE * BY * BX * 4;
 constexpr int ST1_BYTES = r128(H1 * W1 * 4);
 constexpr int NST = 2;
-constexpr int SMEM_BYTES = NST * STAGE_BYTES + 4 * ST1_BYTES + 64;
+constexpr int SMEM_BYTES = NST * STAGE_BYTES + ST1_BYTES + 64;   // + tau_xy (the others live in the stage)
 constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;
 
 // FP32 fields of an instance (each LD32 x rows floats)
@@ -102,11 +102,8 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
     typedef float Row1[W1];
     typedef float RowH[TW];
     typedef float RowT[BX];
-    Row1* sPn = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES);
-    Row1* sTxx = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + ST1_BYTES);
-    Row1* sTyy = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + 2 * ST1_BYTES);
-    Row1* sTxy = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES + 3 * ST1_BYTES);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NST * STAGE_BYTES + 4 * ST1_BYTES);
+    Row1* sTxy = reinterpret_cast<Row1*>(smem + NST * STAGE_BYTES);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + NST * STAGE_BYTES + ST1_BYTES);
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
     const int ntiles = *ntiles_ptr;
@@ -202,6 +199,11 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         const bool interior = i0 > 0 && j0 > 0 && i0 + BX + 2 < Nx && j0 + BY + 2 < Ny;
 
         // ---- stage 1: P and tau of the correction on tile + 1 halo ----
+        // stage 2 needs P only through differences next to tau_xx / tau_yy, so stage 1 keeps
+        // sigma_xx = tau_xx - P (over the divV-residual box) and sigma_yy = tau_yy - P (over the old P box), each
+        // point reading only its own entry of those first, and writes P straight out
+        RowH* sSxx = sRdiv;
+        RowH* sSyy = sPo;
         auto stage1 = [&](int a, int b) {
             const int i = i0 + a, j = j0 + b;
             if (interior || (i < Nx - 1 && j < Ny - 1)) {
@@ -210,9 +212,10 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
                 float div_d = dVx_dx + dVy_dy;
                 float div_full = div_d + sRdiv[b][a];          // divV of V_k + dV
                 float mu = sMup[b][a];
-                sPn[b][a] = sPo[b][a] - c_pt * mu * div_full;
-                sTxx[b][a] = 2.0f * mu * (dVx_dx - (1.0f / 3.0f) * div_d);
-                sTyy[b][a] = 2.0f * mu * (dVy_dy - (1.0f / 3.0f) * div_d);
+                float pn = sPo[b][a] - c_pt * mu * div_full;
+                sSxx[b][a] = 2.0f * mu * (dVx_dx - (1.0f / 3.0f) * div_d) - pn;
+                sSyy[b][a] = 2.0f * mu * (dVy_dy - (1.0f / 3.0f) * div_d) - pn;
+                if (a < BX && b < BY) P_out[a + b * ldi] = pn;
             }
             if (interior || (i < Nx && j < Ny)) {
                 float dVx_dy = (sVx[b + 1][a] - sVx[b][a]) * _dy;
@@ -231,8 +234,7 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         }
         // ---- stage 2: damped rates and velocity update of the correction ----
         auto rate_x = [&](int a, int b, int o) {
-            float Rx = (sTxx[b][a + 1] - sTxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy -
-                       (sPn[b][a + 1] - sPn[b][a]) * _dx + sRx[b][a];
+            float Rx = (sSxx[b][a + 1] - sSxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy + sRx[b][a];
             float dv = dampX * sRvx[b][a] + Rx;
             Rvx[o] = dv;
             float dtau = dmax ? __fdividef(c_vsc, fmaxf(fmaxf(sMup[b][a], sMup[b][a + 1]),
@@ -244,8 +246,7 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
             float av = 0.25f * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
             float dxr = sRho[b + 1][a + 2] - sRho[b + 1][a];
             float dyr = sRho[b + 2][a + 1] - sRho[b][a + 1];
-            float Ry = (sTyy[b + 1][a] - sTyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx -
-                       (sPn[b + 1][a] - sPn[b][a]) * _dy -
+            float Ry = (sSyy[b + 1][a] - sSyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx -
                        g_dt * (av * dxr * 0.5f * _dx + sVy[b + 1][a + 1] * dyr * 0.5f * _dy) + sRy[b][a];
             float dv = dampY * sRvy[b][a] + Ry;
             Rvy[o] = dv;
@@ -259,7 +260,6 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
             for (int r = 0; r < RPT; ++r) {
                 const int a = tx, b = ty + r * TY;
                 const int o = a + b * ldi;
-                P_out[o] = sPn[b][a];
                 Vx_out[o + 1 + ldi] = rate_x(a, b, o);
                 Vy_out[o + 1 + ldi] = rate_y(a, b, o);
             }
@@ -270,7 +270,6 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
                 const int i = i0 + a, j = j0 + b;
                 if (i >= Nx - 1 || j >= Ny - 1) continue;
                 const int o = a + b * ldi;
-                P_out[o] = sPn[b][a];
                 if (i < Nx - 2) {
                     float vn = rate_x(a, b, o);
                     Vx_out[o + 1 + ldi] = vn;

@@ -7,7 +7,7 @@
 //
 //   * the domain is cut into BX x BY tiles of points (i, j), 0 <= i < Nx-1,
 //     0 <= j < Ny-1 (the pressure index space, which contains the dVx and dVy
-//     index spaces); persistent CTAs (2 per SM) walk the tiles;
+//     index spaces); persistent CTAs (3 per SM) walk the tiles;
 //   * one thread per CTA brings the next tile's old Vx, Vy, rho, P, mu_p, mu_b
 //     (tile + 2 halo) and dVx, dVy (tile) into a second shared-memory stage
 //     with bulk-tensor copies (TMA, mbarrier-completed) while the CTA computes
@@ -16,14 +16,17 @@
 //     (the halo row/column is recomputed by the neighbouring tile, cheaper
 //     than a grid-wide barrier), then the residuals, the damped rates dV and
 //     the new velocities of its tile;
-//   * tau, divV, dtau* are never stored (dtau* is recomputed from mu_p);
+//   * tau and divV are stored only on check iterations; dtauVx, dtauVy are
+//     computed once per solve, as compute_timesteps! does, and streamed in
+//     with the tile (16 B per point instead of 4 FP64 divisions);
 //   * the free-slip ghost rows / columns of the new velocities are written by
 //     the CTAs on the domain edge, in the reference's BC order (:53-56);
 //   * V and P are double-buffered (the iteration is Jacobi-like: every read is
 //     an old value), dV is updated in place.
 //
 // HBM bytes per iteration: read Vx, Vy, P, dVx, dVy, rho, mu_b, mu_p and write
-// Vx, Vy, P, dVx, dVy -- 13 arrays, ~104 * Nx * Ny bytes.
+// Vx, Vy, P, dVx, dVy -- 13 arrays, ~104 * Nx * Ny bytes essential, plus the
+// two dtau arrays read (16 * Nx * Ny).
 //
 // Fields live in a padded internal layout (one leading dimension LD, a
 // multiple of 32 doubles, for every field) packed from / unpacked to the
