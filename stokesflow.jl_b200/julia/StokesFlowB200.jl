@@ -17,7 +17,7 @@ module StokesFlowB200
 
 using CUDA
 
-export bilinearMarkerToGrid!, solveStokes!, moveMarkersRK4!
+export bilinearMarkerToGrid!, solveStokes!, moveMarkersRK4!, solveStokesMixed!
 
 const libsf = joinpath(@__DIR__, "..", "lib", "libstokesflow_b200.so")
 
@@ -87,6 +87,34 @@ function solveStokes!(P, Vx_pad, Vy_pad, œÅ_vy, Œº_b, Œº_p, œÑxx, œÑyy, œÑxy, ‚à
                 dptr(Vx_s), dptr(Vy_s), g_y, dx, dy, Nx, Ny, dt, maxdisp, use_free_surface_stabilization, œµ,
                 print_info, iterMax, stream(), info))
     return info[].dt, info[].T_eff, info[].runtime
+end
+
+# sf_batch_instance: one problem of the mixed-precision / batched solver, results written back
+struct BatchInstance
+    P::Ptr{Cdouble}; Vx_pad::Ptr{Cdouble}; Vy_pad::Ptr{Cdouble}; œÅ_vy::Ptr{Cdouble}; Œº_b::Ptr{Cdouble}
+    Œº_p::Ptr{Cdouble}; Vx_s::Ptr{Cdouble}; Vy_s::Ptr{Cdouble}
+    Nx::Int64; Ny::Int64
+    g_y::Float64; dx::Float64; dy::Float64; dt::Float64; maxdisp::Float64; eps::Float64; rel_tol::Float64
+    use_free_surface_stabilization::Int32; retried::Int32
+    dt_out::Float64; err::Float64; eps_used::Float64
+    inner_iters::Int64; outer_iters::Int64
+    converged::Int32; status::Int32
+    batch_ms::Float64
+end
+
+# The problem of solveStokes! solved by FP32 pseudo-transient sweeps with FP64 defect correction: the same
+# FP64 stopping test, not the same bits.  Returns (dt, err, FP32 sweeps).  rel_tol > 0 replaces œµ by
+# rel_tol * mean|g_y œÅ_vy|.
+function solveStokesMixed!(P, Vx_pad, Vy_pad, œÅ_vy, Œº_b, Œº_p, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp;
+                           use_free_surface_stabilization::Bool=true, œµ=1e-8, rel_tol=0.0)
+    info = Ref{BatchInstance}()
+    check(ccall((:sf_solve_stokes_mixed, libsf), Cint,
+                (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
+                 Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Cdouble, Cdouble, Int64, Int64, Cdouble, Cdouble, Cint, Cdouble,
+                 Cdouble, Ptr{Cvoid}, Ptr{Cvoid}, Ref{BatchInstance}),
+                ctx(), dptr(P), dptr(Vx_pad), dptr(Vy_pad), dptr(œÅ_vy), dptr(Œº_b), dptr(Œº_p), dptr(Vx_s), dptr(Vy_s),
+                g_y, dx, dy, Nx, Ny, dt, maxdisp, use_free_surface_stabilization, œµ, rel_tol, C_NULL, stream(), info))
+    return info[].dt_out, info[].err, info[].inner_iters
 end
 
 # MoveMarkers.jl:15
