@@ -110,6 +110,35 @@ def test_engine_reports_diverging_instance(sf):
     assert p[0].result["status"] == 5 and p[1].result["status"] == 0 and p[1].result["converged"] == 1
 
 
+def test_retry_rescues_a_diverging_layout(sf):
+    """A 0.015-viscosity inclusion overlapping a 4.3 one (57^2 points): the reference's pseudo-time step
+    diverges (non-finite after the first fold); with the default retry the instance restarts from its
+    untouched inputs with the stencil-maximum step and converges -- to the same bits as a solve that used
+    that step from the start, since the restart depends on nothing but the inputs."""
+    from stokesflow_b200 import workloads
+    N = 57
+    m = workloads.InclusionModel(inclusions=[(0.41097438276340365, 0.5557518051240106, 0.1352829024064631,
+                                               0.9281545598641852, 0.01517583353528039),
+                                              (0.43634253798256306, 0.5888521117278834, 0.1352829024064631,
+                                               1.1863722075708387, 4.262449612501063)])
+    st = sf.StokesFlow2D(N, N, 1.0, 1.0, m, marker_density=4, jitter=0.5, seed=0, keep_work_arrays=False)
+    st.deposit()
+    f = (host(st.rho_vy), host(st.mu_b), host(st.mu_p))
+    spec = [(N, N, st.dx, st.dy, f)]
+    runs = {}
+    for name, opts in (("plain", dict(retry_local_max=False)), ("retry", {}), ("local_max", dict(dtau_local_max=True))):
+        arrs, probs = problems(sf, spec)
+        res = sf.solve_stokes_batch_mixed(probs, options=sf.mixed_options(max_sweeps=400_000, **opts))
+        runs[name] = (arrs[0], res[0])
+    assert runs["plain"][1]["status"] == 5 and runs["plain"][1]["retried"] == 0
+    r, l = runs["retry"][1], runs["local_max"][1]
+    assert r["status"] == 0 and r["converged"] == 1 and r["retried"] == 1
+    assert l["converged"] == 1 and l["retried"] == 0
+    assert r["inner_iters"] > l["inner_iters"]            # the diverged attempt's sweeps count too
+    for k in ("Vx_pad", "Vy_pad", "P"):
+        assert torch.equal(runs["retry"][0][k], runs["local_max"][0][k]), k
+
+
 def test_serving_same_alone_and_in_mix(sf):
     from stokesflow_b200 import serving
     reqs = serving.poisson_requests(4, rate=0.0, seed=3, cells=(31, 90), timesteps=(2, 3))
@@ -126,6 +155,31 @@ def test_serving_same_alone_and_in_mix(sf):
         for k in ("P", "Vx", "Vy", "x_m", "y_m"):
             assert np.array_equal(alone.final[k], r.final[k]), f"request {r.rid} {k}"
         assert alone.final["t_tot"] == r.final["t_tot"]
+
+
+def test_serving_admission_by_budget(sf):
+    """A budget that holds about one request's state at a time: the rest wait in arrival order, the peak
+    stays within the budget, and every request ends with the same results as with room for all."""
+    from stokesflow_b200 import serving
+    kw = dict(rate=0.0, seed=9, cells=(40, 60), timesteps=(1, 2))
+    reqs = serving.poisson_requests(3, **kw)
+    biggest = max(serving.state_bytes(r.spec) for r in reqs)
+    opts = sf.mixed_options(fold_every=100)
+    tight = serving.StokesServer(2 * biggest + biggest // 2, engine_share=0.5, keep_final=True, options=opts)
+    s = tight.run(reqs)
+    assert s["completed"] == 3 and s["failed"] == 0
+    assert tight.peak_state <= tight.state_budget
+    assert tight.peak_state < sum(serving.state_bytes(r.spec) for r in reqs)   # they did not all fit at once
+    order = sorted(reqs, key=lambda r: r.t_admit)
+    assert [r.rid for r in order] == [0, 1, 2]
+    tight.close()
+    roomy_reqs = serving.poisson_requests(3, **kw)
+    roomy = serving.StokesServer(1 << 30, keep_final=True, options=opts)
+    roomy.run(roomy_reqs)
+    roomy.close()
+    for a, b in zip(reqs, roomy_reqs):
+        for k in ("P", "Vx", "Vy", "x_m", "y_m"):
+            assert np.array_equal(a.final[k], b.final[k]), f"request {a.rid} {k}"
 
 
 def test_serving_state_bytes_and_fp64_server(sf):
