@@ -69,6 +69,7 @@ class StokesFlow2D:
     solver: str = "fp64"              # "fp64": plain path, bit-identical to the reference; "mixed": FP32 sweeps +
                                       # FP64 defect correction
     mixed_opts: object = None
+    snapshot_dir: str | None = None   # save_to_file: the reference's .mat snapshots at start and after every step
     ctx: api.Context | None = None
     history: list = field(default_factory=list)
 
@@ -127,6 +128,11 @@ class StokesFlow2D:
         self.nt = 0
         self.counts = None
         self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
+        self.snapshots = None
+        if self.snapshot_dir:   # StokesFlow2D_multixpu.jl:136-141: stats, markers and grid before the first step
+            from .snapshots import SnapshotWriter
+            self.snapshots = SnapshotWriter(self.snapshot_dir, self)
+            self.snapshots.snapshot(0)
 
     @property
     def n_markers(self):
@@ -214,9 +220,17 @@ class StokesFlow2D:
         t.d2h_ms = ev[5].elapsed_time(ev[6])
         self.t_tot += self.dt
         self.nt += 1
+        if self.snapshots is not None:   # :194-198, written in the background
+            self.snapshots.snapshot(self.nt)
         rec = dict(nt=self.nt, dt=self.dt, t_tot=self.t_tot, times=t, info=info)
         self.history.append(rec)
         return rec
+
+    def close_snapshots(self):
+        """Wait for the snapshot files still being written."""
+        if self.snapshots is not None:
+            self.snapshots.close()
+            self.snapshots = None
 
     # split timestep for a serving loop: the solve runs in a shared engine between the two halves
     def begin_timestep(self) -> api.MixedProblem:
@@ -259,15 +273,17 @@ def _host(a: torch.Tensor) -> np.ndarray:
 
 def stokes_flow_2d(Nt, Nx, Ny, Lx, Ly, model: api.PlumeModel, *, marker_density=5, stokes_eps=1e-5,
                    stokes_rtol=None, jitter=0.0, seed=0, g_y=9.81, maxdisp=0.5, iter_max=100000, rebin=False,
-                   return_state=False):
+                   save_to_file=False, out_dir="viz_out", return_state=False):
     """StokesFlow2D (StokesFlow2D_multixpu.jl:55-235) on one GPU.
     Returns (Vx_glob, Vy_glob, t_tot) as host arrays (Julia shape, Fortran order)
-    and, with return_state, the StokesFlow2D state object."""
+    and, with return_state, the StokesFlow2D state object.  save_to_file writes the reference's .mat
+    snapshots into out_dir (stats.mat, markers_%04d_0000.mat, grid_%04d_0000.mat)."""
     st = StokesFlow2D(Nx, Ny, float(Lx), float(Ly), model, marker_density=marker_density, stokes_eps=stokes_eps,
                       stokes_rtol=stokes_rtol, jitter=jitter, seed=seed, g_y=g_y, maxdisp=maxdisp,
-                      iter_max=iter_max, rebin=rebin)
+                      iter_max=iter_max, rebin=rebin, snapshot_dir=out_dir if save_to_file else None)
     for _ in range(Nt):
         st.step()
+    st.close_snapshots()
     Vx, Vy = st.velocities_host()
     if return_state:
         return Vx, Vy, st.t_tot, st
