@@ -163,6 +163,47 @@ int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int6
                              double g_y, void* stream, double* scale);
 
 /* ---------------------------------------------------------------------- */
+/* domain decomposition: one solve over a dims_x x dims_y grid of ranks     */
+/* ---------------------------------------------------------------------- */
+/* One rank of a decomposed solve: its context (whose device and work
+ * stream run the rank) and its local arrays, each as in sf_solve_stokes for
+ * the local grid of Nx x Ny points, which overlaps its neighbours by 2
+ * points as ImplicitGlobalGrid's (init_global_grid, overlaps 2). */
+typedef struct {
+    sf_ctx* ctx;
+    double* P;                 /* (Nx-1, Ny-1)  in/out */
+    double* Vx_pad;            /* (Nx+2, Ny+1)  out    */
+    double* Vy_pad;            /* (Nx+1, Ny+2)  out    */
+    const double* rho_vy;      /* (Nx+1, Ny)           */
+    const double* mu_b;        /* (Nx,   Ny)           */
+    const double* mu_p;        /* (Nx-1, Ny-1)         */
+    double* dVxdt;             /* (Nx-2, Ny-1)  in/out */
+    double* dVydt;             /* (Nx-1, Ny-2)  in/out */
+    double* Vx_s;              /* (Nx,   Ny+1)  in/out */
+    double* Vy_s;              /* (Nx+1, Ny)    in/out */
+    int32_t coord_x, coord_y;  /* the rank's position; global point = coord * (N - 2) + local point */
+} sf_domain;
+
+/* Replaces solveStokes! run on dims_x * dims_y MPI ranks
+ * (StokesSolver_multixpu.jl:14-96 with update_halo! at :57 and :93, the
+ * Allreduce of compute_err :103-109 and compute_dt :118-121), driven from
+ * one host thread over the ranks' devices (one GPU per rank, or several
+ * ranks on one GPU).  The global grid is nx_g = dims_x (Nx-2) + 2 by
+ * ny_g = dims_y (Ny-2) + 2 points, and the constants (damping, max_nxy,
+ * ncheck, ndtupdate) use it.  Each iteration every rank runs the fused
+ * kernel on its local grid (free-slip BCs on its local edges, as the
+ * reference's BC kernels do), then the first / last planes of Vx_s and Vy_s
+ * are copied from the neighbours (x then y, so corners follow).  The
+ * iterates are bit-identical to a single-domain solve of the global grid.
+ * err is the reference's multi-rank value: the mean over ranks of each rank's
+ * local mean |Rx|, |Ry|, |divV| (overlap points counted by each rank).
+ * info (may be NULL) receives the global results.  Synchronous. */
+int sf_solve_stokes_decomposed(sf_domain* domains, int32_t dims_x, int32_t dims_y, int64_t Nx, int64_t Ny,
+                               double g_y, double dx, double dy, double dt, double maxdisp,
+                               int use_free_surface_stabilization, double eps, int64_t iter_max,
+                               sf_solve_info* info);
+
+/* ---------------------------------------------------------------------- */
 /* mixed-precision and batched solves (no reference counterpart: the       */
 /* reference has only the FP64 solveStokes!)                                */
 /* ---------------------------------------------------------------------- */

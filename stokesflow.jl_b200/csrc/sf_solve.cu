@@ -39,7 +39,10 @@
 // the file is compiled with -fmad=false: the iterates are bit-identical to
 // the reference's (only the summation order inside the residual norm differs).
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
+#include <cstring>
+#include <functional>
 #include <vector>
 
 #include "sf_internal.cuh"
@@ -688,49 +691,20 @@ struct Solver {
     }
 };
 
-}  // namespace sf
+// the caller's arrays of one solve, in sf_solve_stokes's order (the work arrays may be NULL)
+struct SolveArgs {
+    double *P, *Vx_pad, *Vy_pad;
+    const double *rho_vy, *mu_b, *mu_p;
+    double *txx, *tyy, *txy, *divV, *dtPt, *Rx, *Ry, *dVxdt, *dVydt, *dtVx, *dtVy, *Vx_s, *Vy_s;
+};
 
-using namespace sf;
-
-extern "C" {
-
-int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int64_t Ny, double g_y, void* stream,
-                             double* scale) {
-    SF_REQUIRE(ctx && rho_vy && scale, "sf_stokes_residual_scale: NULL argument");
-    SF_REQUIRE(Nx >= 3 && Ny >= 3, "sf_stokes_residual_scale: grid too small");
-    int rc = set_device(ctx);
-    if (rc) return rc;
-    cudaStream_t s = as_stream(stream);
-    int nb = (int)std::min<int64_t>(ceil_div((Nx - 1) * (Ny - 2), 256), 1024);
-    if ((rc = ensure(ctx, ctx->partials, (size_t)nb * 8))) return rc;
-    k_rho_scale<<<nb, 256, 0, s>>>(rho_vy, (int)Nx, (int)Ny, g_y, (double*)ctx->partials.ptr);
-    SF_LAUNCHED(ctx);
-    k_sum_partials<<<1, 1024, 0, s>>>((double*)ctx->partials.ptr, nb, (double)((Nx - 1) * (Ny - 2)),
-                                      ctx->d_scalars + SC_SCALE);
-    SF_LAUNCHED(ctx);
-    SF_CUDA(cudaMemcpyAsync(ctx->h_scalars + SC_SCALE, ctx->d_scalars + SC_SCALE, 8, cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaStreamSynchronize(s));
-    *scale = ctx->h_scalars[SC_SCALE];
-    return SF_OK;
-}
-
-int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy, const double* mu_b,
-                    const double* mu_p, double* txx, double* tyy, double* txy, double* divV, double* dtPt, double* Rx,
-                    double* Ry, double* dVxdt, double* dVydt, double* dtVx, double* dtVy, double* Vx_s, double* Vy_s,
-                    double g_y, double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
-                    int use_stab, double eps, int print_info, int64_t iter_max, void* stream, sf_solve_info* info) {
-    SF_REQUIRE(ctx, "sf_solve_stokes: ctx is NULL");
-    SF_REQUIRE(Nx >= 4 && Ny >= 4, "sf_solve_stokes: Nx, Ny must be >= 4");
-    SF_REQUIRE(Nx < (1 << 20) && Ny < (1 << 20), "sf_solve_stokes: Nx, Ny too large");
-    SF_REQUIRE(P && Vx_pad && Vy_pad && rho_vy && mu_b && mu_p && dVxdt && dVydt && Vx_s && Vy_s,
-               "sf_solve_stokes: a state / parameter array is NULL");
-    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_solve_stokes: dx, dy must be positive");
-    int rc = set_device(ctx);
-    if (rc) return rc;
-    cudaStream_t s = as_stream(stream);
-
-    // ---- layout / scratch ----
-    Solver S;
+// Layout, scratch, pack, compute_timesteps! and kernel parameters of one (local) grid of Nx x Ny points.
+// nx_g, ny_g are the global grid sizes the reference's constants use (nx_g(), ny_g(): :20-22): the local
+// ones on a single domain.
+static int solver_prepare(Solver& S, sf_ctx* ctx, cudaStream_t s, const SolveArgs& A, int64_t Nx, int64_t Ny,
+                          double g_y, double dx, double dy, double dt, double maxdisp, int use_stab, int64_t nx_g,
+                          int64_t ny_g) {
+    int rc;
     S.ctx = ctx;
     S.s = s;
     S.L.Nx = Nx;
@@ -754,20 +728,17 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     const double Vdmp = 4.0, Vsc = 0.45, Ptsc = 1.0 / 2.0;
     const double mdxy = std::min(dx, dy);
     const double min_dxy2 = mdxy * mdxy;
-    const double max_nxy = (double)std::max(Nx, Ny);
-    const double dampX = 1.0 - Vdmp / (double)Nx;
-    const double dampY = 1.0 - Vdmp / (double)Ny;
+    const double max_nxy = (double)std::max(nx_g, ny_g);
+    const double dampX = 1.0 - Vdmp / (double)nx_g;
+    const double dampY = 1.0 - Vdmp / (double)ny_g;
     if (!use_stab) dt = 0.0;  // :29-31
-    const int64_t mnxy = std::min(Nx, Ny);
-    const int64_t ncheck = std::min<int64_t>(5 * mnxy, 2000);  // :35
-    const int64_t ndtupdate = 10 * mnxy;                       // :36
 
     // ---- pack ----
     const int64_t LD = S.L.LD;
     struct Pk { int f; const double* src; int64_t nx, ny; } packs[] = {
-        {F_VXA, Vx_s, Nx, Ny + 1}, {F_VYA, Vy_s, Nx + 1, Ny}, {F_PA, P, Nx - 1, Ny - 1},
-        {F_DVX, dVxdt, Nx - 2, Ny - 1}, {F_DVY, dVydt, Nx - 1, Ny - 2}, {F_RHO, rho_vy, Nx + 1, Ny},
-        {F_MUB, mu_b, Nx, Ny}, {F_MUP, mu_p, Nx - 1, Ny - 1}};
+        {F_VXA, A.Vx_s, Nx, Ny + 1}, {F_VYA, A.Vy_s, Nx + 1, Ny}, {F_PA, A.P, Nx - 1, Ny - 1},
+        {F_DVX, A.dVxdt, Nx - 2, Ny - 1}, {F_DVY, A.dVydt, Nx - 1, Ny - 2}, {F_RHO, A.rho_vy, Nx + 1, Ny},
+        {F_MUB, A.mu_b, Nx, Ny}, {F_MUP, A.mu_p, Nx - 1, Ny - 1}};
     for (const Pk& k : packs) {
         k_copy2d<<<copy_blocks(ctx, k.nx * k.ny), 256, 0, s>>>(S.L.f(k.f), LD, k.src, k.nx, k.nx, k.ny);
         SF_LAUNCHED(ctx);
@@ -781,10 +752,11 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
                                                                      S.L.f(F_DTVX), LD, S.L.f(F_DTVY), LD,
                                                                      nullptr, 0);
     SF_LAUNCHED(ctx);
-    if (dtVx || dtVy || dtPt) {
+    if (A.dtVx || A.dtVy || A.dtPt) {
         k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
-                                                                         Vsc * min_dxy2, Ptsc * 4.1, max_nxy, dtVx,
-                                                                         Nx - 2, dtVy, Nx - 1, dtPt, Nx - 1);
+                                                                         Vsc * min_dxy2, Ptsc * 4.1, max_nxy,
+                                                                         A.dtVx, Nx - 2, A.dtVy, Nx - 1, A.dtPt,
+                                                                         Nx - 1);
         SF_LAUNCHED(ctx);
     }
 
@@ -835,6 +807,194 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     rp._dx = pt._dx;
     rp._dy = pt._dy;
     rp.g_y = g_y;
+    return SF_OK;
+}
+
+// :89-93: the state back into the caller's arrays, Vx_pad / Vy_pad with the mirrored ghost planes
+static int solver_unpack(Solver& S, const SolveArgs& A, int64_t niter, int64_t nchecks) {
+    sf_ctx* ctx = S.ctx;
+    cudaStream_t s = S.s;
+    const int64_t Nx = S.L.Nx, Ny = S.L.Ny, LD = S.L.LD;
+    struct Uk { double* dst; const double* src; int64_t nx, ny; } unpacks[] = {
+        {A.Vx_s, S.Vx_cur(), Nx, Ny + 1}, {A.Vy_s, S.Vy_cur(), Nx + 1, Ny}, {A.P, S.P_cur(), Nx - 1, Ny - 1},
+        {A.dVxdt, S.L.f(F_DVX), Nx - 2, Ny - 1}, {A.dVydt, S.L.f(F_DVY), Nx - 1, Ny - 2},
+        {A.txx, S.L.f(F_TXX), Nx - 1, Ny - 1}, {A.tyy, S.L.f(F_TYY), Nx - 1, Ny - 1}, {A.txy, S.L.f(F_TXY), Nx, Ny},
+        {A.divV, S.L.f(F_DIV), Nx - 1, Ny - 1},
+        {nchecks ? A.Rx : nullptr, S.L.f(F_RX), Nx - 2, Ny - 1}, {nchecks ? A.Ry : nullptr, S.L.f(F_RY), Nx - 1, Ny - 2}};
+    for (const Uk& k : unpacks) {
+        if (!k.dst || niter == 0 && (k.src == S.L.f(F_TXX) || k.src == S.L.f(F_TYY) || k.src == S.L.f(F_TXY) ||
+                                     k.src == S.L.f(F_DIV)))
+            continue;
+        k_copy2d<<<copy_blocks(ctx, k.nx * k.ny), 256, 0, s>>>(k.dst, k.nx, k.src, LD, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    k_pad_vx<<<copy_blocks(ctx, (Nx + 2) * (Ny + 1)), 256, 0, s>>>(A.Vx_pad, S.Vx_cur(), LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    k_pad_vy<<<copy_blocks(ctx, (Nx + 1) * (Ny + 2)), 256, 0, s>>>(A.Vy_pad, S.Vy_cur(), LD, (int)Nx, (int)Ny);
+    SF_LAUNCHED(ctx);
+    return SF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// domain decomposition: update_halo! of ImplicitGlobalGrid (overlap 2) between ranks driven by one thread
+// ---------------------------------------------------------------------------
+struct Rank {
+    sf_ctx* ctx;
+    cudaStream_t s;
+    cudaEvent_t ev;     // the rank's last finished phase (kernel, x halos, y halos)
+    int left, right, down, up;  // neighbour ranks, -1 at a physical boundary
+    Solver S;
+    SolveArgs A;
+};
+
+// one array of every rank for a halo update: entry (i, j) at p[r] + i + j * ld[r]; local size (Nx + sx, Ny + sy)
+struct HaloArray {
+    std::vector<double*> p;
+    std::vector<int64_t> ld;
+    int64_t sx, sy;
+};
+
+// ImplicitGlobalGrid's overlap of an array along a dimension: the grid overlap (2) plus how much the array is
+// larger than the grid there.  With ol = 2 + s and n = N + s entries, the last plane n-1 of a rank is the plane
+// ol-1 of its upper neighbour, and the neighbour's first plane 0 is the rank's plane n-ol (0-based).
+static int halo_dimension(std::vector<Rank>& R, const std::vector<HaloArray>& arrays, int dim, int64_t Nx,
+                          int64_t Ny) {
+    for (size_t r = 0; r < R.size(); ++r) {
+        const int up = dim == 0 ? R[r].right : R[r].up;
+        if (up < 0) continue;
+        Rank& a = R[r];
+        Rank& b = R[up];
+        for (const HaloArray& h : arrays) {
+            const int64_t nx = Nx + h.sx, ny = Ny + h.sy, n = dim == 0 ? nx : ny, ol = 2 + (dim == 0 ? h.sx : h.sy);
+            // into b's first plane from a's plane n-ol, on b's stream once a's phase is done
+            auto plane = [&](const double* src, int64_t ld_src, int64_t i_src, double* dst, int64_t ld_dst,
+                             int64_t i_dst, cudaStream_t s) -> int {
+                if (dim == 0)
+                    SF_CUDA(cudaMemcpy2DAsync(dst + i_dst, ld_dst * 8, src + i_src, ld_src * 8, 8, ny,
+                                              cudaMemcpyDefault, s));
+                else
+                    SF_CUDA(cudaMemcpyAsync(dst + i_dst * ld_dst, src + i_src * ld_src, nx * 8, cudaMemcpyDefault, s));
+                return SF_OK;
+            };
+            int rc;
+            SF_CUDA(cudaSetDevice(b.ctx->device));
+            SF_CUDA(cudaStreamWaitEvent(b.s, a.ev, 0));
+            if ((rc = plane(h.p[r], h.ld[r], n - ol, h.p[up], h.ld[up], 0, b.s))) return rc;
+            // into a's last plane from b's plane ol-1, on a's stream once b's phase is done
+            SF_CUDA(cudaSetDevice(a.ctx->device));
+            SF_CUDA(cudaStreamWaitEvent(a.s, b.ev, 0));
+            if ((rc = plane(h.p[up], h.ld[up], ol - 1, h.p[r], h.ld[r], n - 1, a.s))) return rc;
+        }
+    }
+    for (Rank& k : R) {  // this dimension's incoming planes are in place
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        SF_CUDA(cudaEventRecord(k.ev, k.s));
+    }
+    return SF_OK;
+}
+
+static int update_halos(std::vector<Rank>& R, const std::vector<HaloArray>& arrays, int64_t Nx, int64_t Ny) {
+    int rc = halo_dimension(R, arrays, 0, Nx, Ny);
+    if (!rc) rc = halo_dimension(R, arrays, 1, Nx, Ny);
+    return rc;
+}
+
+// the current Vx_s, Vy_s of every rank in the padded layout
+static std::vector<HaloArray> state_halos(std::vector<Rank>& R) {
+    HaloArray vx{{}, {}, 0, 1}, vy{{}, {}, 1, 0};
+    for (Rank& k : R) {
+        vx.p.push_back(const_cast<double*>(k.S.Vx_cur()));
+        vx.ld.push_back(k.S.L.LD);
+        vy.p.push_back(const_cast<double*>(k.S.Vy_cur()));
+        vy.ld.push_back(k.S.L.LD);
+    }
+    return {vx, vy};
+}
+
+// compute_dt over all ranks (:118-121 with the MIN Allreduce): maxdisp * min(dx / max|Vx|, dy / max|Vy|) with the
+// maxima over every rank's local arrays; the division is monotone and correctly rounded, so this is the
+// reference's min over ranks of the local values
+static int global_dt(std::vector<Rank>& R, double maxdisp, double dx, double dy, double* dt) {
+    for (Rank& k : R) {
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        int rc = k.S.compute_dt(-1, -1);
+        if (rc) return rc;
+        SF_CUDA(cudaMemcpyAsync(k.ctx->h_scalars + SC_MAX_VX, k.ctx->d_scalars + SC_MAX_VX, 2 * 8,
+                                cudaMemcpyDeviceToHost, k.s));
+    }
+    double mvx = 0.0, mvy = 0.0;
+    bool nan = false;
+    for (Rank& k : R) {
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        SF_CUDA(cudaStreamSynchronize(k.s));
+        const double a = k.ctx->h_scalars[SC_MAX_VX], b = k.ctx->h_scalars[SC_MAX_VY];
+        nan = nan || a != a || b != b;
+        mvx = std::max(mvx, a);
+        mvy = std::max(mvy, b);
+    }
+    const double a = dx / mvx, b = dy / mvy;
+    double m = (b < a) ? b : a;
+    *dt = nan ? std::nan("") : maxdisp * m;
+    return SF_OK;
+}
+
+static int set_scalar_all(std::vector<Rank>& R, int slot, double v) {
+    for (Rank& k : R) {
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        k_set_scalar<<<1, 1, 0, k.s>>>(k.ctx->d_scalars + slot, v);
+        SF_LAUNCHED(k.ctx);
+    }
+    return SF_OK;
+}
+
+}  // namespace sf
+
+using namespace sf;
+
+extern "C" {
+
+int sf_stokes_residual_scale(sf_ctx* ctx, const double* rho_vy, int64_t Nx, int64_t Ny, double g_y, void* stream,
+                             double* scale) {
+    SF_REQUIRE(ctx && rho_vy && scale, "sf_stokes_residual_scale: NULL argument");
+    SF_REQUIRE(Nx >= 3 && Ny >= 3, "sf_stokes_residual_scale: grid too small");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    int nb = (int)std::min<int64_t>(ceil_div((Nx - 1) * (Ny - 2), 256), 1024);
+    if ((rc = ensure(ctx, ctx->partials, (size_t)nb * 8))) return rc;
+    k_rho_scale<<<nb, 256, 0, s>>>(rho_vy, (int)Nx, (int)Ny, g_y, (double*)ctx->partials.ptr);
+    SF_LAUNCHED(ctx);
+    k_sum_partials<<<1, 1024, 0, s>>>((double*)ctx->partials.ptr, nb, (double)((Nx - 1) * (Ny - 2)),
+                                      ctx->d_scalars + SC_SCALE);
+    SF_LAUNCHED(ctx);
+    SF_CUDA(cudaMemcpyAsync(ctx->h_scalars + SC_SCALE, ctx->d_scalars + SC_SCALE, 8, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaStreamSynchronize(s));
+    *scale = ctx->h_scalars[SC_SCALE];
+    return SF_OK;
+}
+
+int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy, const double* mu_b,
+                    const double* mu_p, double* txx, double* tyy, double* txy, double* divV, double* dtPt, double* Rx,
+                    double* Ry, double* dVxdt, double* dVydt, double* dtVx, double* dtVy, double* Vx_s, double* Vy_s,
+                    double g_y, double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
+                    int use_stab, double eps, int print_info, int64_t iter_max, void* stream, sf_solve_info* info) {
+    SF_REQUIRE(ctx, "sf_solve_stokes: ctx is NULL");
+    SF_REQUIRE(Nx >= 4 && Ny >= 4, "sf_solve_stokes: Nx, Ny must be >= 4");
+    SF_REQUIRE(Nx < (1 << 20) && Ny < (1 << 20), "sf_solve_stokes: Nx, Ny too large");
+    SF_REQUIRE(P && Vx_pad && Vy_pad && rho_vy && mu_b && mu_p && dVxdt && dVydt && Vx_s && Vy_s,
+               "sf_solve_stokes: a state / parameter array is NULL");
+    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_solve_stokes: dx, dy must be positive");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+
+    Solver S;
+    const SolveArgs A{P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt,
+                      dtVx, dtVy, Vx_s, Vy_s};
+    if ((rc = solver_prepare(S, ctx, s, A, Nx, Ny, g_y, dx, dy, dt, maxdisp, use_stab, Nx, Ny))) return rc;
+    const int64_t mnxy = std::min(Nx, Ny);
+    const int64_t ncheck = std::min<int64_t>(5 * mnxy, 2000);  // :35
+    const int64_t ndtupdate = 10 * mnxy;                       // :36
 
     // ---- PT loop (:43-77) ----
     double err = 2.0 * eps;
@@ -879,23 +1039,7 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     SF_CUDA(cudaEventRecord(ctx->ev_b, s));
 
     // ---- unpack (:89-95) ----
-    struct Uk { double* dst; const double* src; int64_t nx, ny; } unpacks[] = {
-        {Vx_s, S.Vx_cur(), Nx, Ny + 1}, {Vy_s, S.Vy_cur(), Nx + 1, Ny}, {P, S.P_cur(), Nx - 1, Ny - 1},
-        {dVxdt, S.L.f(F_DVX), Nx - 2, Ny - 1}, {dVydt, S.L.f(F_DVY), Nx - 1, Ny - 2},
-        {txx, S.L.f(F_TXX), Nx - 1, Ny - 1}, {tyy, S.L.f(F_TYY), Nx - 1, Ny - 1}, {txy, S.L.f(F_TXY), Nx, Ny},
-        {divV, S.L.f(F_DIV), Nx - 1, Ny - 1},
-        {nchecks ? Rx : nullptr, S.L.f(F_RX), Nx - 2, Ny - 1}, {nchecks ? Ry : nullptr, S.L.f(F_RY), Nx - 1, Ny - 2}};
-    for (const Uk& k : unpacks) {
-        if (!k.dst || niter == 0 && (k.src == S.L.f(F_TXX) || k.src == S.L.f(F_TYY) || k.src == S.L.f(F_TXY) ||
-                                     k.src == S.L.f(F_DIV)))
-            continue;
-        k_copy2d<<<copy_blocks(ctx, k.nx * k.ny), 256, 0, s>>>(k.dst, k.nx, k.src, LD, k.nx, k.ny);
-        SF_LAUNCHED(ctx);
-    }
-    k_pad_vx<<<copy_blocks(ctx, (Nx + 2) * (Ny + 1)), 256, 0, s>>>(Vx_pad, S.Vx_cur(), LD, (int)Nx, (int)Ny);
-    SF_LAUNCHED(ctx);
-    k_pad_vy<<<copy_blocks(ctx, (Nx + 1) * (Ny + 2)), 256, 0, s>>>(Vy_pad, S.Vy_cur(), LD, (int)Nx, (int)Ny);
-    SF_LAUNCHED(ctx);
+    if ((rc = solver_unpack(S, A, niter, nchecks))) return rc;
     if ((rc = S.compute_dt(SC_DT_OUT, -1))) return rc;  // returned dt (:95)
     SF_CUDA(cudaMemcpyAsync(ctx->h_scalars, ctx->d_scalars, SC_N * 8, cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
@@ -934,6 +1078,160 @@ int sf_solve_stokes(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, cons
     SF_CUDA(cudaMemcpy(&hflag, ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
     if (hflag) return fail(SF_ERR_CUDA, "sf_solve_stokes: a tile copy into shared memory did not complete in time");
     if (!(err == err) || std::isinf(err)) return fail(SF_ERR_NONFINITE, "sf_solve_stokes: residual is not finite");
+    return SF_OK;
+}
+
+int sf_solve_stokes_decomposed(sf_domain* domains, int32_t dims_x, int32_t dims_y, int64_t Nx, int64_t Ny,
+                               double g_y, double dx, double dy, double dt, double maxdisp, int use_stab, double eps,
+                               int64_t iter_max, sf_solve_info* info) {
+    SF_REQUIRE(domains && dims_x >= 1 && dims_y >= 1 && dims_x * dims_y <= 4096, "sf_solve_stokes_decomposed: bad dims");
+    SF_REQUIRE(Nx >= 4 && Ny >= 4 && Nx < (1 << 20) && Ny < (1 << 20), "sf_solve_stokes_decomposed: bad local grid");
+    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_solve_stokes_decomposed: dx, dy must be positive");
+    const int nr = dims_x * dims_y;
+    std::vector<int> at((size_t)nr, -1);  // rank index of each coordinate
+    for (int r = 0; r < nr; ++r) {
+        const sf_domain& d = domains[r];
+        SF_REQUIRE(d.ctx && d.P && d.Vx_pad && d.Vy_pad && d.rho_vy && d.mu_b && d.mu_p && d.dVxdt && d.dVydt &&
+                       d.Vx_s && d.Vy_s,
+                   "sf_solve_stokes_decomposed: a domain array is NULL");
+        SF_REQUIRE(d.coord_x >= 0 && d.coord_x < dims_x && d.coord_y >= 0 && d.coord_y < dims_y,
+                   "sf_solve_stokes_decomposed: coordinate outside dims");
+        const int c = d.coord_x + d.coord_y * dims_x;
+        SF_REQUIRE(at[c] < 0, "sf_solve_stokes_decomposed: two domains have the same coordinates");
+        at[c] = r;
+    }
+    const int64_t nx_g = (int64_t)dims_x * (Nx - 2) + 2, ny_g = (int64_t)dims_y * (Ny - 2) + 2;  // nx_g(), ny_g()
+    const int64_t mnxy = std::min(nx_g, ny_g);
+    const int64_t ncheck = std::min<int64_t>(5 * mnxy, 2000);  // :35
+    const int64_t ndtupdate = 10 * mnxy;                       // :36
+    if (!use_stab) dt = 0.0;
+
+    std::vector<Rank> R((size_t)nr);
+    int rc;
+    for (int r = 0; r < nr; ++r) {
+        const sf_domain& d = domains[r];
+        Rank& k = R[r];
+        k.ctx = d.ctx;
+        if ((rc = set_device(k.ctx))) return rc;
+        SF_CUDA(cudaDeviceSynchronize());  // the caller's inputs are complete
+        k.s = k.ctx->work;
+        SF_CUDA(cudaEventCreateWithFlags(&k.ev, cudaEventDisableTiming));
+        auto nb = [&](int cx, int cy) { return (cx < 0 || cy < 0 || cx >= dims_x || cy >= dims_y) ? -1 : at[cx + cy * dims_x]; };
+        k.left = nb(d.coord_x - 1, d.coord_y);
+        k.right = nb(d.coord_x + 1, d.coord_y);
+        k.down = nb(d.coord_x, d.coord_y - 1);
+        k.up = nb(d.coord_x, d.coord_y + 1);
+        k.A = SolveArgs{d.P, d.Vx_pad, d.Vy_pad, d.rho_vy, d.mu_b, d.mu_p, nullptr, nullptr, nullptr, nullptr, nullptr,
+                        nullptr, nullptr, d.dVxdt, d.dVydt, nullptr, nullptr, d.Vx_s, d.Vy_s};
+        if ((rc = solver_prepare(k.S, k.ctx, k.s, k.A, Nx, Ny, g_y, dx, dy, dt, maxdisp, use_stab, nx_g, ny_g)))
+            return rc;
+        SF_CUDA(cudaEventRecord(k.ev, k.s));
+    }
+    auto destroy_events = [&]() {
+        for (Rank& k : R)
+            if (k.ev) {
+                cudaSetDevice(k.ctx->device);
+                cudaEventDestroy(k.ev);
+            }
+    };
+    struct Guard { std::function<void()> f; ~Guard() { f(); } } guard{destroy_events};
+
+    // ---- PT loop (:43-77), every rank per iteration, halos after it (:57) ----
+    const auto t0 = std::chrono::steady_clock::now();
+    double err = 2.0 * eps;
+    int64_t iter = 1, niter = 0, nchecks = 0;
+    while (err > eps && iter <= iter_max) {
+        const bool store = (iter % ncheck == 0) || (iter == iter_max);
+        for (Rank& k : R) {
+            SF_CUDA(cudaSetDevice(k.ctx->device));
+            // the neighbours have finished reading this rank's planes of the previous iteration
+            for (int n : {k.left, k.right, k.down, k.up})
+                if (n >= 0) SF_CUDA(cudaStreamWaitEvent(k.s, R[n].ev, 0));
+        }
+        for (Rank& k : R) {
+            SF_CUDA(cudaSetDevice(k.ctx->device));
+            if ((rc = k.S.launch_iter(store))) return rc;
+            SF_CUDA(cudaEventRecord(k.ev, k.s));
+        }
+        if ((rc = update_halos(R, state_halos(R), Nx, Ny))) return rc;
+        const bool dt_up = use_stab && (iter % ndtupdate == 0);
+        const bool check = (iter % ncheck == 0);
+        if (dt_up || (check && use_stab)) {  // :59-61, :64-68
+            double d_new = 0.0;
+            if ((rc = global_dt(R, maxdisp, dx, dy, &d_new))) return rc;
+            if (dt_up && (rc = set_scalar_all(R, SC_DT, d_new))) return rc;
+            if (check && (rc = set_scalar_all(R, SC_DT_CHECK, d_new))) return rc;
+        } else if (check) {
+            if ((rc = set_scalar_all(R, SC_DT_CHECK, 0.0))) return rc;
+        }
+        if (check) {  // :69-70, compute_err with the SUM Allreduce of the local means (:103-109)
+            for (Rank& k : R) {
+                SF_CUDA(cudaSetDevice(k.ctx->device));
+                if ((rc = k.S.residuals())) return rc;
+                SF_CUDA(cudaMemcpyAsync(k.ctx->h_scalars + SC_SUM_RX, k.ctx->d_scalars + SC_SUM_RX, 3 * 8,
+                                        cudaMemcpyDeviceToHost, k.s));
+            }
+            double mean[3] = {0.0, 0.0, 0.0};
+            const double cnt[3] = {(double)(Nx - 2) * (Ny - 1), (double)(Nx - 1) * (Ny - 2), (double)(Nx - 1) * (Ny - 1)};
+            for (Rank& k : R) {
+                SF_CUDA(cudaSetDevice(k.ctx->device));
+                SF_CUDA(cudaStreamSynchronize(k.s));
+                for (int q = 0; q < 3; ++q) mean[q] += k.ctx->h_scalars[SC_SUM_RX + q] / cnt[q];
+            }
+            for (int q = 0; q < 3; ++q) mean[q] /= (double)nr;
+            double m = mean[0];
+            if (mean[1] > m || mean[1] != mean[1]) m = mean[1];
+            if (mean[2] > m || mean[2] != mean[2]) m = mean[2];
+            if (mean[0] != mean[0]) m = mean[0];
+            err = m;
+            ++nchecks;
+            for (Rank& k : R) {
+                SF_CUDA(cudaSetDevice(k.ctx->device));
+                SF_CUDA(cudaEventRecord(k.ev, k.s));
+            }
+        }
+        ++niter;
+        ++iter;
+        if (!(err == err) || std::isinf(err)) break;
+    }
+
+    // ---- unpack, Vx_pad / Vy_pad mirrored and their halos updated (:89-93) ----
+    HaloArray px{{}, {}, 2, 1}, py{{}, {}, 1, 2};
+    for (Rank& k : R) {
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        for (int n : {k.left, k.right, k.down, k.up})
+            if (n >= 0) SF_CUDA(cudaStreamWaitEvent(k.s, R[n].ev, 0));
+        if ((rc = solver_unpack(k.S, k.A, niter, nchecks))) return rc;
+        SF_CUDA(cudaEventRecord(k.ev, k.s));
+        px.p.push_back(k.A.Vx_pad);
+        px.ld.push_back(Nx + 2);
+        py.p.push_back(k.A.Vy_pad);
+        py.ld.push_back(Nx + 1);
+    }
+    if ((rc = update_halos(R, {px, py}, Nx, Ny))) return rc;
+    double dt_out = 0.0;
+    if ((rc = global_dt(R, maxdisp, dx, dy, &dt_out))) return rc;  // :95
+    int hflag = 0;
+    for (Rank& k : R) {
+        SF_CUDA(cudaSetDevice(k.ctx->device));
+        SF_CUDA(cudaStreamSynchronize(k.s));
+        int f = 0;
+        SF_CUDA(cudaMemcpy(&f, k.ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost));
+        hflag |= f;
+    }
+    const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (info) {
+        memset(info, 0, sizeof(*info));
+        info->dt = dt_out;
+        info->iters = niter;
+        info->err = err;
+        info->n_checks = nchecks;
+        info->converged = (err <= eps) ? 1 : 0;
+        info->loop_ms = ms;
+        info->fused_launches = niter * nr;
+    }
+    if (hflag) return fail(SF_ERR_CUDA, "sf_solve_stokes_decomposed: a tile copy into shared memory did not complete in time");
+    if (!(err == err) || std::isinf(err)) return fail(SF_ERR_NONFINITE, "sf_solve_stokes_decomposed: residual is not finite");
     return SF_OK;
 }
 

@@ -83,6 +83,12 @@ class EngineStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Domain(C.Structure):
+    """sf_domain."""
+    _fields_ = [(n, _vp) for n in ("ctx", "P", "Vx_pad", "Vy_pad", "rho_vy", "mu_b", "mu_p", "dVxdt", "dVydt",
+                                    "Vx_s", "Vy_s")] + [("coord_x", _i32), ("coord_y", _i32)]
+
+
 class PlumeModelC(C.Structure):
     """sf_plume_model."""
     _fields_ = [(n, _d) for n in ("air_height", "plume_x", "plume_y", "plume_r", "rho_air", "rho_matrix",
@@ -105,6 +111,8 @@ PROTOTYPES = {
     "sf_solve_stokes": (C.c_int, [_vp] + [_pd] * 19 + [_d, _d, _d, _i64, _i64, _d, _d, C.c_int, _d, C.c_int, _i64,
                                                        _vp, C.POINTER(SolveInfo)]),
     "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),
+    "sf_solve_stokes_decomposed": (C.c_int, [C.POINTER(Domain), _i32, _i32, _i64, _i64, _d, _d, _d, _d, _d, C.c_int,
+                                             _d, _i64, C.POINTER(SolveInfo)]),
     "sf_solve_stokes_batch_mixed": (C.c_int, [_vp, C.POINTER(BatchInstance), C.c_int, C.POINTER(MixedOptions), _vp]),
     "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64, _d, _d,
                                         C.c_int, _d, _d, C.POINTER(MixedOptions), _vp, C.POINTER(BatchInstance)]),

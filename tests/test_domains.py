@@ -1,0 +1,78 @@
+"""Domain decomposition of the PT solve (sf_solve_stokes_decomposed): the ImplicitGlobalGrid index
+arithmetic on the CPU, and on the GPU the decomposed iterate against the single-domain one, bit for bit,
+with every rank's local arrays (halos and overlaps included) equal to the slices of the global result."""
+import numpy as np
+import pytest
+import torch
+
+from fields import random_fields
+from stokesflow_b200 import domains
+
+
+def test_sizes_and_slices_tile_the_global_grid():
+    for dims, n_local in ((1, 10), (2, 34), (3, 18), (4, 6)):
+        n_g = domains.global_size(dims, n_local)
+        assert domains.local_size(dims, n_g) == n_local
+    with pytest.raises(ValueError):
+        domains.local_size(3, 66)            # 64 does not split in 3
+    Nx, Ny, dims = 6, 5, (3, 2)
+    nx_g, ny_g = domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)
+    for name, (sx, sy) in domains.ARRAYS.items():
+        cover = np.zeros((nx_g + sx, ny_g + sy), dtype=int)
+        for cy in range(dims[1]):
+            for cx in range(dims[0]):
+                xs, ys = domains.local_slices(name, (cx, cy), Nx, Ny)
+                assert xs.stop - xs.start == Nx + sx and ys.stop - ys.start == Ny + sy
+                cover[xs, ys] += 1
+        assert cover.min() >= 1, name               # every global entry is held by some rank
+        assert cover[-1, -1] == 1 and cover[0, 0] == 1
+
+
+def test_split_keeps_the_overlap_consistent():
+    Nx, Ny, dims = 8, 6, (2, 2)
+    nx_g, ny_g = domains.global_size(2, Nx), domains.global_size(2, Ny)
+    g = torch.arange(float(nx_g * (ny_g + 1)), dtype=torch.float64).reshape(ny_g + 1, nx_g).t()   # Vx_s layout
+    loc = domains.split({"Vx_s": g}, dims, Nx, Ny)
+    a, b = loc[(0, 0)]["Vx_s"], loc[(1, 0)]["Vx_s"]
+    assert a.stride() == (1, a.shape[0])
+    assert torch.equal(a[-2:, :], b[:2, :])         # the two overlapping x planes
+    c = loc[(0, 1)]["Vx_s"]
+    assert torch.equal(a[:, -3:], c[:, :3])         # Vx_s is one entry longer in y: three planes overlap
+
+
+def _global_problem(sf, nx_g, ny_g, seed=4):
+    rho, mub, mup = random_fields(nx_g, ny_g, seed=seed, contrast=10.0)
+    rng = np.random.default_rng(seed + 1)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).cuda().t()  # noqa: E731
+    z = sf.zeros
+    g = {"rho_vy": dev(rho), "mu_b": dev(mub), "mu_p": dev(mup), "P": dev(1e-3 * rng.standard_normal((nx_g - 1, ny_g - 1))),
+         "Vx_s": dev(1e-3 * rng.standard_normal((nx_g, ny_g + 1))), "Vy_s": dev(1e-3 * rng.standard_normal((nx_g + 1, ny_g))),
+         "dVxdt": z(nx_g - 2, ny_g - 1), "dVydt": z(nx_g - 1, ny_g - 2), "Vx_pad": z(nx_g + 2, ny_g + 1),
+         "Vy_pad": z(nx_g + 1, ny_g + 2)}
+    return g
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(1, 1), (2, 1), (2, 2), (3, 2)])
+def test_decomposed_solve_is_the_global_solve(sf, dims):
+    nx_g, ny_g = 74, 50
+    Nx, Ny = domains.local_size(dims[0], nx_g), domains.local_size(dims[1], ny_g)
+    g = _global_problem(sf, nx_g, ny_g)
+    ranks = domains.split(g, dims, Nx, Ny)          # copies of the initial state
+    dx, dy = 1.0 / (nx_g - 1), 1.0 / (ny_g - 1)
+    iters = 600                                      # checks at 250 and 500, a dt update at 500
+    info = sf.solve_stokes_info(g["P"], g["Vx_pad"], g["Vy_pad"], g["rho_vy"], g["mu_b"], g["mu_p"], None, None, None,
+                                None, None, None, None, g["dVxdt"], g["dVydt"], None, None, g["Vx_s"], g["Vy_s"], 9.81,
+                                dx, dy, nx_g, ny_g, 1e-4, 0.5, eps=1e-300, iter_max=iters)
+    dinfo = domains.solve_stokes_decomposed(ranks, dims, Nx, Ny, 9.81, dx, dy, 1e-4, 0.5, eps=1e-300, iter_max=iters)
+    torch.cuda.synchronize()
+    assert dinfo["iters"] == info["iters"] == iters and dinfo["n_checks"] == info["n_checks"] == 2
+    assert dinfo["dt"] == info["dt"]
+    if dims == (1, 1):
+        assert dinfo["err"] == info["err"]
+    else:   # the reference's multi-rank err averages per-rank means: close, not equal
+        assert abs(dinfo["err"] - info["err"]) <= 0.5 * info["err"]
+    for coord, loc in ranks.items():
+        for name in domains.ARRAYS:
+            xs, ys = domains.local_slices(name, coord, Nx, Ny)
+            assert torch.equal(loc[name], g[name][xs, ys]), f"rank {coord} {name}"
