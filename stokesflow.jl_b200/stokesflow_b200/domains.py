@@ -50,7 +50,9 @@ def split(global_arrays: dict, dims, Nx: int, Ny: int) -> dict:
             for name, a in global_arrays.items():
                 xs, ys = local_slices(name, (cx, cy), Nx, Ny)
                 v = a[xs, ys]
-                loc[name] = v.t().contiguous().t()   # column-major like the library's arrays
+                # always a copy (a whole-array slice of a 1-rank split would otherwise share storage),
+                # column-major like the library's arrays
+                loc[name] = v.t().clone().t()
             out[(cx, cy)] = loc
     return out
 

@@ -35,6 +35,8 @@ def test_split_keeps_the_overlap_consistent():
     loc = domains.split({"Vx_s": g}, dims, Nx, Ny)
     a, b = loc[(0, 0)]["Vx_s"], loc[(1, 0)]["Vx_s"]
     assert a.stride() == (1, a.shape[0])
+    whole = domains.split({"Vx_s": g}, (1, 1), nx_g, ny_g)[(0, 0)]["Vx_s"]
+    assert torch.equal(whole, g) and whole.data_ptr() != g.data_ptr()   # a copy, never a view
     assert torch.equal(a[-2:, :], b[:2, :])         # the two overlapping x planes
     c = loc[(0, 1)]["Vx_s"]
     assert torch.equal(a[:, -3:], c[:, :3])         # Vx_s is one entry longer in y: three planes overlap
