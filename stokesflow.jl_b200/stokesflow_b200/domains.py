@@ -57,6 +57,45 @@ def split(global_arrays: dict, dims, Nx: int, Ny: int) -> dict:
     return out
 
 
+def gather(ranks: dict, name: str, dims, Nx: int, Ny: int) -> torch.Tensor:
+    """The global array `name` from the ranks' local ones, as gather_V_grid / create_grid_view assemble it
+    (GlobalGather.jl:59-114): along each dimension the overlap o = 2 + s (s: extra entries of the array)
+    splits at every rank boundary, o//2 entries dropped from the lower rank and the rest from the upper."""
+    sx, sy = ARRAYS[name]
+    some = next(iter(ranks.values()))[name]
+    out = torch.empty((global_size(dims[0], Nx) + sx, global_size(dims[1], Ny) + sy), dtype=some.dtype,
+                      device=some.device)
+
+    def kept(c, dimsn, n_loc, s):
+        o = 2 + s
+        nl = o // 2
+        nr = o - nl
+        lo = nr if c > 0 else 0
+        hi = n_loc + s - nl if c < dimsn - 1 else n_loc + s
+        return lo, hi, c * (n_loc - 2)
+
+    for (cx, cy), loc in ranks.items():
+        x_lo, x_hi, x0 = kept(cx, dims[0], Nx, sx)
+        y_lo, y_hi, y0 = kept(cy, dims[1], Ny, sy)
+        out[x0 + x_lo:x0 + x_hi, y0 + y_lo:y0 + y_hi] = loc[name][x_lo:x_hi, y_lo:y_hi]
+    return out
+
+
+def gather_markers(ranks_markers: dict, dims, lx_loc: float, ly_loc: float, dx: float, dy: float):
+    """gather_markers! (GlobalGather.jl:10-48): the ranks' markers concatenated in MPI rank order of the
+    Cartesian communicator (x coordinate slowest), each shifted from local to global coordinates by
+    (coord_x (lx_loc - dx), coord_y (ly_loc - dy)).  ranks_markers: {(cx, cy): (x_m, y_m, rho_m, mu_m)}."""
+    xs, ys, rs, ms = [], [], [], []
+    for cx in range(dims[0]):
+        for cy in range(dims[1]):
+            x, y, r, m = ranks_markers[(cx, cy)]
+            xs.append(x + cx * (lx_loc - dx))
+            ys.append(y + cy * (ly_loc - dy))
+            rs.append(r)
+            ms.append(m)
+    return torch.cat(xs), torch.cat(ys), torch.cat(rs), torch.cat(ms)
+
+
 def solve_stokes_decomposed(ranks: dict, dims, Nx: int, Ny: int, g_y, dx, dy, dt, maxdisp, *, eps=1e-8,
                             iter_max=100000, use_free_surface_stabilization=True, contexts=None) -> dict:
     """solveStokes! on dims[0] x dims[1] ranks (StokesSolver_multixpu.jl:14-96 with update_halo! and the

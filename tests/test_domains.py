@@ -42,6 +42,33 @@ def test_split_keeps_the_overlap_consistent():
     assert torch.equal(a[:, -3:], c[:, :3])         # Vx_s is one entry longer in y: three planes overlap
 
 
+def test_gather_inverts_split():
+    """With consistent overlaps (as after update_halo!) the gathered array is the global one, for every
+    staggering; the kept ranges tile each dimension without gaps."""
+    Nx, Ny, dims = 7, 6, (3, 2)
+    nx_g, ny_g = domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)
+    g = {}
+    for name, (sx, sy) in domains.ARRAYS.items():
+        g[name] = torch.randn(ny_g + sy, nx_g + sx, dtype=torch.float64).t()
+    loc = domains.split(g, dims, Nx, Ny)
+    for name in domains.ARRAYS:
+        assert torch.equal(domains.gather(loc, name, dims, Nx, Ny), g[name]), name
+
+
+def test_gather_markers_order_and_shift():
+    dims, lx, ly, dx, dy = (2, 2), 1.0, 0.5, 0.25, 0.125
+    mk = {}
+    for cx in range(2):
+        for cy in range(2):
+            base = 10 * cx + cy
+            mk[(cx, cy)] = (torch.tensor([0.1, 0.2], dtype=torch.float64), torch.tensor([0.3, 0.4], dtype=torch.float64),
+                            torch.tensor([base, base], dtype=torch.float64), torch.tensor([1.0, 2.0], dtype=torch.float64))
+    x, y, r, m = domains.gather_markers(mk, dims, lx, ly, dx, dy)
+    assert r.tolist() == [0, 0, 1, 1, 10, 10, 11, 11]          # rank order: x coordinate slowest
+    assert x.tolist()[4:6] == [0.1 + 1 * (lx - dx), 0.2 + 1 * (lx - dx)]
+    assert y.tolist()[2:4] == [0.3 + 1 * (ly - dy), 0.4 + 1 * (ly - dy)]
+
+
 def _global_problem(sf, nx_g, ny_g, seed=4):
     rho, mub, mup = random_fields(nx_g, ny_g, seed=seed, contrast=10.0)
     rng = np.random.default_rng(seed + 1)
@@ -78,3 +105,5 @@ def test_decomposed_solve_is_the_global_solve(sf, dims):
         for name in domains.ARRAYS:
             xs, ys = domains.local_slices(name, coord, Nx, Ny)
             assert torch.equal(loc[name], g[name][xs, ys]), f"rank {coord} {name}"
+    for name in ("Vx_pad", "Vy_pad", "P"):   # what gather_V_grid hands back
+        assert torch.equal(domains.gather(ranks, name, dims, Nx, Ny), g[name]), name
