@@ -203,6 +203,59 @@ int sf_solve_stokes_decomposed(sf_domain* domains, int32_t dims_x, int32_t dims_
                                int use_free_surface_stabilization, double eps, int64_t iter_max,
                                sf_solve_info* info);
 
+/* One rank's array for sf_sum_overlapping_values: nx x ny entries, column-major, on the context's device. */
+typedef struct {
+    sf_ctx* ctx;
+    double* a;
+    int32_t coord_x, coord_y;
+} sf_rank_array;
+
+/* Replaces sumOverlappingValues!(A, grid) (MarkerToGrid.jl:183-269): the
+ * entries each rank shares with a neighbour (ox = 2 + nx - Nx planes in x,
+ * oy = 2 + ny - Ny in y) become the sum of both ranks' values, x first and
+ * then y (so corners collect all four), each as own + received.  Used by the
+ * decomposed deposit on val_wt_sum and wt_sum.  Synchronous. */
+int sf_sum_overlapping_values(sf_rank_array* ranks, int32_t dims_x, int32_t dims_y, int64_t Nx, int64_t Ny,
+                              int64_t nx, int64_t ny);
+
+/* safeDivision over a grid (MarkerToGrid.jl:164-172, launched on 1:nx x
+ * 1:ny at :35): val_grid[i,j] = val_wt_sum[i,j] / wt_sum[i,j] where the
+ * weight is not 0; elsewhere val_grid keeps its value and the node is counted
+ * as empty (sf_warnings.empty_nodes).  The sums have leading dimension ld_sum
+ * (the reference's interpolation arrays are (Nx+1, Ny) for every grid). */
+int sf_safe_division(sf_ctx* ctx, double* val_grid, int64_t nx, int64_t ny, const double* val_wt_sum,
+                     const double* wt_sum, int64_t ld_sum, void* stream);
+
+/* One rank of a marker exchange: its markers before (x, y, rho, mu; n of
+ * them), its output arrays (capacity entries each) and, on return, n_out. */
+typedef struct {
+    sf_ctx* ctx;
+    const double* x;
+    const double* y;
+    const double* rho;
+    const double* mu;
+    int64_t n;
+    double* x_out;
+    double* y_out;
+    double* rho_out;
+    double* mu_out;
+    int64_t capacity;
+    int64_t n_out;             /* result: markers after the exchange */
+    int32_t coord_x, coord_y;
+} sf_marker_rank;
+
+/* Replaces exchangeMarkers (MarkerExchange.jl:8-163) for all ranks of a
+ * dims_x x dims_y grid, driven from one thread.  A marker within half a cell
+ * (dx/2, dy/2) of an edge shared with a neighbour goes to that neighbour
+ * (posToNeighbourIdx, :204-222, eight neighbours), its position shifted by
+ * (lx - dx, ly - dy) per step; the output is the rank's kept markers in their
+ * order, then the received ones by neighbour index 1..8 (:60-90, :150-157),
+ * each in the sender's order.  The inputs are not modified.  If some rank's
+ * capacity is too small, nothing is written, every n_out holds the size
+ * needed and the call returns SF_ERR_TOO_LARGE.  Synchronous. */
+int sf_exchange_markers(sf_marker_rank* ranks, int32_t dims_x, int32_t dims_y, double lx, double ly, double dx,
+                        double dy);
+
 /* ---------------------------------------------------------------------- */
 /* mixed-precision and batched solves (no reference counterpart: the       */
 /* reference has only the FP64 solveStokes!)                                */

@@ -284,3 +284,81 @@ def stokes_flow_2d(Nt, Nx, Ny, Lx, Ly, model: PlumeModel, marker_density=5, stok
     if return_state:
         return a["Vx"], a["Vy"], t_tot, dict(arrays=a, x_m=x_m, y_m=y_m, rho_m=rho_m, mu_m=mu_m, iters=iters)
     return a["Vx"], a["Vy"], t_tot
+
+
+# --------------------------------------------------------------------------
+# decomposed run: the pieces that cross ranks (numpy restatements)
+# --------------------------------------------------------------------------
+def sum_overlapping_values(arrays: dict, dims, Nx: int, Ny: int) -> None:
+    """sumOverlappingValues!(A, grid) (scripts/MarkerToGrid.jl:183-269) on numpy arrays in the Julia shape,
+    keyed by rank coordinates (cx, cy): the x exchange first (:223-246), then y (:249-266); every received
+    block holds the neighbour's values from before that pass, added as own + received (A .+= recv)."""
+    nx, ny = next(iter(arrays.values())).shape
+    ox, oy = 2 + nx - Nx, 2 + ny - Ny
+    assert 2 * ox <= nx and 2 * oy <= ny                                   # :199
+    if ox > 0:
+        recv = {}
+        for (cx, cy) in arrays:
+            left, right = arrays.get((cx - 1, cy)), arrays.get((cx + 1, cy))
+            recv[(cx, cy)] = (None if left is None else left[nx - ox:, :].copy(),
+                              None if right is None else right[:ox, :].copy())
+        for c, A in arrays.items():
+            lr, rl = recv[c]
+            if lr is not None:
+                A[:ox, :] += lr
+            if rl is not None:
+                A[nx - ox:, :] += rl
+    if oy > 0:
+        recv = {}
+        for (cx, cy) in arrays:
+            above, below = arrays.get((cx, cy - 1)), arrays.get((cx, cy + 1))   # nb[1,2] / nb[2,2]
+            recv[(cx, cy)] = (None if above is None else above[:, ny - oy:].copy(),
+                              None if below is None else below[:, :oy].copy())
+        for c, A in arrays.items():
+            down, up = recv[c]
+            if down is not None:
+                A[:, :oy] += down
+            if up is not None:
+                A[:, ny - oy:] += up
+
+
+_SHIFT = {1: (-1, -1), 2: (0, -1), 3: (1, -1), 4: (1, 0), 5: (1, 1), 6: (0, 1), 7: (-1, 1), 8: (-1, 0)}
+
+
+def _pos_to_neighbour_idx(x, y, lx, ly, hx, hy, cx, cy, dimx, dimy):
+    """posToNeighbourIdx (scripts/MarkerExchange.jl:204-222), vectorised; the conditions in its order."""
+    d = np.zeros(x.shape, dtype=np.int64)
+    lo_y, hi_y = (y < hy) & (cy != 0), (y > ly - hy) & (cy != dimy - 1)
+    lo_x, hi_x = (x < hx) & (cx != 0), (x > lx - hx) & (cx != dimx - 1)
+    d = np.where(lo_y, np.where(lo_x, 1, np.where(hi_x, 3, 2)),
+                 np.where(hi_y, np.where(lo_x, 7, np.where(hi_x, 5, 6)),
+                          np.where(lo_x, 8, np.where(hi_x, 4, 0))))
+    return d
+
+
+def exchange_markers(markers: dict, dims, lx, ly, dx, dy) -> dict:
+    """exchangeMarkers (scripts/MarkerExchange.jl:8-163) for every rank: markers {(cx, cy): (x, y, rho, mu)}
+    -> the same after the exchange.  A rank keeps its inside markers in order (:60-76) and appends, for
+    neighbour index i = 1..8, the markers that the rank opposite direction i (dstToSrcIdx, :198-202) sent
+    in direction i, shifted by (lx - dx, ly - dy) times the step (:77-79), in the sender's order."""
+    hx, hy = dx / 2, dy / 2
+    dimx, dimy = dims
+    kept, sent = {}, {}
+    for (cx, cy), (x, y, r, m) in markers.items():
+        d = _pos_to_neighbour_idx(x, y, lx, ly, hx, hy, cx, cy, dimx, dimy)
+        k = d == 0
+        kept[(cx, cy)] = (x[k], y[k], r[k], m[k])
+        for i, (sx, sy) in _SHIFT.items():
+            s = d == i
+            sent[((cx, cy), i)] = (x[s] - (lx - dx) * sx, y[s] - (ly - dy) * sy, r[s], m[s])
+    out = {}
+    for (cx, cy) in markers:
+        parts = [kept[(cx, cy)]]
+        for i in range(1, 9):
+            src_dir = i + 4 if i < 5 else (i + 4) % 9 + 1
+            sx, sy = _SHIFT[src_dir]
+            src = (cx + sx, cy + sy)
+            if src in markers:
+                parts.append(sent[(src, i)])
+        out[(cx, cy)] = tuple(np.concatenate([p[q] for p in parts]) for q in range(4))
+    return out

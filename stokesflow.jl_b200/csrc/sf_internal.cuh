@@ -67,6 +67,8 @@ struct sf_ctx {
     sf::Scratch keys, counts, offsets, cursor, perm, scan_tmp;
     // PT solve: padded internal fields, reduction partials; mixed/batched engine arena
     sf::Scratch fields, partials, mixed;
+    // decomposed timestep: marker-exchange and overlap-sum staging
+    sf::Scratch exch;
     cudaStream_t work = nullptr;  // private non-blocking stream (graph capture needs a non-legacy stream)
     // device counters (unsigned long long[CNT_N]) and scalars (double[SC_N])
     unsigned long long* d_counters = nullptr;
@@ -85,6 +87,15 @@ int ensure(sf_ctx* ctx, Scratch& s, size_t bytes);
 int set_device(sf_ctx* ctx);
 // frees the context's cached batch engine (sf_mixed.cu)
 void mixed_engine_release(sf_ctx* ctx);
+
+// true when no two of the n contexts (reached through get(i)) are the same: a rank's scratch is its own
+template <typename Get>
+bool distinct_contexts(int n, Get get) {
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j)
+            if (get(i) == get(j)) return false;
+    return true;
+}
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }

@@ -1088,6 +1088,8 @@ int sf_solve_stokes_decomposed(sf_domain* domains, int32_t dims_x, int32_t dims_
     SF_REQUIRE(Nx >= 4 && Ny >= 4 && Nx < (1 << 20) && Ny < (1 << 20), "sf_solve_stokes_decomposed: bad local grid");
     SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_solve_stokes_decomposed: dx, dy must be positive");
     const int nr = dims_x * dims_y;
+    SF_REQUIRE(distinct_contexts(nr, [&](int i) { return domains[i].ctx; }),
+               "sf_solve_stokes_decomposed: every rank needs its own context");
     std::vector<int> at((size_t)nr, -1);  // rank index of each coordinate
     for (int r = 0; r < nr; ++r) {
         const sf_domain& d = domains[r];

@@ -89,6 +89,18 @@ class Domain(C.Structure):
                                     "Vx_s", "Vy_s")] + [("coord_x", _i32), ("coord_y", _i32)]
 
 
+class RankArray(C.Structure):
+    """sf_rank_array."""
+    _fields_ = [("ctx", _vp), ("a", _vp), ("coord_x", _i32), ("coord_y", _i32)]
+
+
+class MarkerRank(C.Structure):
+    """sf_marker_rank."""
+    _fields_ = [("ctx", _vp), ("x", _vp), ("y", _vp), ("rho", _vp), ("mu", _vp), ("n", _i64), ("x_out", _vp),
+                ("y_out", _vp), ("rho_out", _vp), ("mu_out", _vp), ("capacity", _i64), ("n_out", _i64),
+                ("coord_x", _i32), ("coord_y", _i32)]
+
+
 class PlumeModelC(C.Structure):
     """sf_plume_model."""
     _fields_ = [(n, _d) for n in ("air_height", "plume_x", "plume_y", "plume_r", "rho_air", "rho_matrix",
@@ -113,6 +125,9 @@ PROTOTYPES = {
     "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),
     "sf_solve_stokes_decomposed": (C.c_int, [C.POINTER(Domain), _i32, _i32, _i64, _i64, _d, _d, _d, _d, _d, C.c_int,
                                              _d, _i64, C.POINTER(SolveInfo)]),
+    "sf_sum_overlapping_values": (C.c_int, [C.POINTER(RankArray), _i32, _i32, _i64, _i64, _i64, _i64]),
+    "sf_safe_division": (C.c_int, [_vp, _pd, _i64, _i64, _pd, _pd, _i64, _vp]),
+    "sf_exchange_markers": (C.c_int, [C.POINTER(MarkerRank), _i32, _i32, _d, _d, _d, _d]),
     "sf_solve_stokes_batch_mixed": (C.c_int, [_vp, C.POINTER(BatchInstance), C.c_int, C.POINTER(MixedOptions), _vp]),
     "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64, _d, _d,
                                         C.c_int, _d, _d, C.POINTER(MixedOptions), _vp, C.POINTER(BatchInstance)]),

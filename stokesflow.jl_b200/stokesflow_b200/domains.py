@@ -96,6 +96,82 @@ def gather_markers(ranks_markers: dict, dims, lx_loc: float, ly_loc: float, dx: 
     return torch.cat(xs), torch.cat(ys), torch.cat(rs), torch.cat(ms)
 
 
+def _ordered(d: dict):
+    return sorted(d.items(), key=lambda kv: (kv[0][1], kv[0][0]))
+
+
+def sum_overlapping_values(arrays: dict, dims, Nx: int, Ny: int, contexts: dict):
+    """sumOverlappingValues! (MarkerToGrid.jl:183-269) over all ranks: arrays {(cx, cy): column-major CUDA
+    tensor}, all of one shape; contexts {(cx, cy): api.Context}, one per rank."""
+    from .api import _grid
+    arr = (_lib.RankArray * len(arrays))()
+    shape = None
+    for k, (coord, a) in enumerate(_ordered(arrays)):
+        shape = tuple(a.shape)
+        arr[k].ctx = contexts[coord].handle
+        arr[k].a = _grid(a, "array", shape)
+        arr[k].coord_x, arr[k].coord_y = int(coord[0]), int(coord[1])
+    check(lib().sf_sum_overlapping_values(arr, int(dims[0]), int(dims[1]), int(Nx), int(Ny), shape[0], shape[1]),
+          "sum_overlapping_values")
+
+
+def deposit_decomposed(x_grid_min, y_grid_min, val_grids: dict, markers: dict, dx, dy, dims, Nx: int, Ny: int,
+                       contexts: dict, sums: dict | None = None):
+    """bilinearMarkerToGrid! on every rank (MarkerToGrid.jl:18-38): each rank's markers summed onto its own
+    grid, the weight and value sums added across the overlaps (sumOverlappingValues! on the (Nx+1, Ny)
+    interpolation arrays, StokesFlow2D_multixpu.jl:112-114), then safeDivision.  val_grids {(cx, cy): grid},
+    markers {(cx, cy): (x_m, y_m, val_m)} in local coordinates; sums: reusable {(cx, cy): (val_wt_sum,
+    wt_sum)} of shape (Nx+1, Ny)."""
+    from . import api
+    if sums is None:
+        sums = {c: (api.zeros(Nx + 1, Ny, device=g.device), api.zeros(Nx + 1, Ny, device=g.device))
+                for c, g in val_grids.items()}
+    for coord, g in val_grids.items():
+        x, y, v = markers[coord]
+        vws, ws = sums[coord]
+        api.bilinear_marker_to_grid(x_grid_min, y_grid_min, g, x, y, v, dx, dy, vws, ws, ctx=contexts[coord])
+    sum_overlapping_values({c: s[1] for c, s in sums.items()}, dims, Nx, Ny, contexts)
+    sum_overlapping_values({c: s[0] for c, s in sums.items()}, dims, Nx, Ny, contexts)
+    for coord, g in val_grids.items():
+        vws, ws = sums[coord]
+        check(lib().sf_safe_division(contexts[coord].handle, api._grid(g, "val_grid"), g.shape[0], g.shape[1],
+                                     vws.data_ptr(), ws.data_ptr(), vws.shape[0], api._stream(None)),
+              "safe_division")
+    return sums
+
+
+def exchange_markers(markers: dict, dims, lx, ly, dx, dy, contexts: dict) -> dict:
+    """exchangeMarkers (MarkerExchange.jl:8-163) for all ranks: markers {(cx, cy): (x, y, rho, mu)} in local
+    coordinates -> the same after the exchange (new tensors): kept markers in order, then the received ones
+    by neighbour index 1..8."""
+    ranks = _ordered(markers)
+    arr = (_lib.MarkerRank * len(ranks))()
+    outs = {}
+
+    def fill(cap_of):
+        for k, (coord, (x, y, r, m)) in enumerate(ranks):
+            cap = cap_of(coord, x.numel())
+            o = [torch.empty(max(cap, 1), dtype=torch.float64, device=x.device) for _ in range(4)]
+            outs[coord] = o
+            d = arr[k]
+            d.ctx = contexts[coord].handle
+            d.x, d.y, d.rho, d.mu = x.data_ptr(), y.data_ptr(), r.data_ptr(), m.data_ptr()
+            d.n = x.numel()
+            d.x_out, d.y_out, d.rho_out, d.mu_out = (t.data_ptr() for t in o)
+            d.capacity = cap
+            d.coord_x, d.coord_y = int(coord[0]), int(coord[1])
+
+    torch.cuda.synchronize()
+    fill(lambda coord, n: n + n // 8 + 1024)
+    st = lib().sf_exchange_markers(arr, int(dims[0]), int(dims[1]), float(lx), float(ly), float(dx), float(dy))
+    if st == _lib.SF_ERR_TOO_LARGE:   # more arrived than the first guess holds: size exactly and redo
+        need = {coord: arr[k].n_out for k, (coord, _) in enumerate(ranks)}
+        fill(lambda coord, n: need[coord])
+        st = lib().sf_exchange_markers(arr, int(dims[0]), int(dims[1]), float(lx), float(ly), float(dx), float(dy))
+    check(st, "exchange_markers")
+    return {coord: tuple(t[:arr[k].n_out] for t in outs[coord]) for k, (coord, _) in enumerate(ranks)}
+
+
 def solve_stokes_decomposed(ranks: dict, dims, Nx: int, Ny: int, g_y, dx, dy, dt, maxdisp, *, eps=1e-8,
                             iter_max=100000, use_free_surface_stabilization=True, contexts=None) -> dict:
     """solveStokes! on dims[0] x dims[1] ranks (StokesSolver_multixpu.jl:14-96 with update_halo! and the
