@@ -172,6 +172,62 @@ def exchange_markers(markers: dict, dims, lx, ly, dx, dy, contexts: dict) -> dic
     return {coord: tuple(t[:arr[k].n_out] for t in outs[coord]) for k, (coord, _) in enumerate(ranks)}
 
 
+class DecomposedStokesFlow2D:
+    """The StokesFlow2D timestep loop (StokesFlow2D_multixpu.jl:157-191) on dims[0] x dims[1] ranks driven from
+    this process: per timestep the three deposits with overlap sums, the decomposed solve, RK4 advection of
+    each rank's markers on its local domain, and the marker exchange.  Nx, Ny: local grid points of a rank;
+    Lx, Ly: the global domain.  markers {(cx, cy): (x_m, y_m, rho_m, mu_m)} in local coordinates (the ranks'
+    initial markers); devices {(cx, cy): CUDA device index} (default: the current device for all)."""
+
+    def __init__(self, dims, Nx: int, Ny: int, Lx: float, Ly: float, markers: dict, *, eps=1e-5, iter_max=100000,
+                 g_y=9.81, maxdisp=0.5, devices: dict | None = None):
+        from . import api
+        from .driver import node_origins
+        self.dims, self.Nx, self.Ny = tuple(dims), Nx, Ny
+        self.dx = Lx / (global_size(dims[0], Nx) - 1)    # :76-77 with nx_g()
+        self.dy = Ly / (global_size(dims[1], Ny) - 1)
+        self.lx, self.ly = (Nx - 1) * self.dx, (Ny - 1) * self.dy
+        self.o = node_origins(self.dx, self.dy)
+        self.eps, self.iter_max, self.g_y, self.maxdisp = eps, iter_max, g_y, maxdisp
+        self.dt, self.t_tot, self.nt = 0.0, 0.0, 0
+        self.ctx, self.ranks, self.sums = {}, {}, {}
+        coords = [(cx, cy) for cy in range(dims[1]) for cx in range(dims[0])]
+        for c in coords:
+            dev = (devices or {}).get(c, torch.cuda.current_device())
+            with torch.cuda.device(dev):
+                self.ctx[c] = api.Context(dev)
+                z = lambda *s: api.zeros(*s, device=f"cuda:{dev}")  # noqa: E731
+                self.ranks[c] = {n: z(Nx + sx, Ny + sy) for n, (sx, sy) in ARRAYS.items()}
+                self.sums[c] = (z(Nx + 1, Ny), z(Nx + 1, Ny))   # interp_size (:112-114)
+        self.markers = {c: tuple(t.to(f"cuda:{self.ranks[c]['P'].device.index}") for t in markers[c]) for c in coords}
+
+    def step(self) -> dict:
+        from . import api
+        d, o = self.dims, self.o
+        Nx, Ny = self.Nx, self.Ny
+        for name, (xo, yo), q in (("rho_vy", ("x_rho", "y_rho"), 2), ("mu_b", ("x", "y"), 3),
+                                  ("mu_p", ("x_p", "y_p"), 3)):          # :164-166
+            grids = {c: r[name] for c, r in self.ranks.items()}
+            mk = {c: (m[0], m[1], m[q]) for c, m in self.markers.items()}
+            deposit_decomposed(o[xo], o[yo], grids, mk, self.dx, self.dy, d, Nx, Ny, self.ctx, self.sums)
+        info = solve_stokes_decomposed(self.ranks, d, Nx, Ny, self.g_y, self.dx, self.dy, self.dt, self.maxdisp,
+                                       eps=self.eps, iter_max=self.iter_max, contexts=self.ctx)   # :171-176
+        self.dt = info["dt"]
+        for c, r in self.ranks.items():                                   # :181, on the local domain
+            x, y = self.markers[c][0], self.markers[c][1]
+            api.move_markers_rk4(x, y, r["Vx_pad"], r["Vy_pad"], o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"],
+                                 self.dt, self.lx, self.ly, self.dx, self.dy, ctx=self.ctx[c])
+        self.markers = exchange_markers(self.markers, d, self.lx, self.ly, self.dx, self.dy, self.ctx)   # :186-191
+        self.t_tot += self.dt
+        self.nt += 1
+        return dict(nt=self.nt, dt=self.dt, t_tot=self.t_tot, info=info)
+
+    def velocities(self):
+        """(Vx_glob, Vy_glob) as gather_V_grid hands them back (StokesFlow2D_multixpu.jl:232)."""
+        return (gather(self.ranks, "Vx_pad", self.dims, self.Nx, self.Ny),
+                gather(self.ranks, "Vy_pad", self.dims, self.Nx, self.Ny))
+
+
 def solve_stokes_decomposed(ranks: dict, dims, Nx: int, Ny: int, g_y, dx, dy, dt, maxdisp, *, eps=1e-8,
                             iter_max=100000, use_free_surface_stabilization=True, contexts=None) -> dict:
     """solveStokes! on dims[0] x dims[1] ranks (StokesSolver_multixpu.jl:14-96 with update_halo! and the

@@ -106,3 +106,84 @@ def test_overlap_sum_and_decomposed_deposit_match_oracle(sf):
         nz = ws[c] != 0
         expect[nz] = vws[c][nz] / ws[c][nz]
         assert np.array_equal(grids[c].cpu().numpy(), expect), c
+
+
+def _initial_markers(dims, Nx, Ny, dx, dy, per_rank, seed):
+    """Seeded markers of every rank inside its own part of the domain (half a cell clear of the edges shared
+    with a neighbour, as the reference's layout keeps them), with smooth rho / mu of the global position."""
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    rng = np.random.default_rng(seed)
+    out = {}
+    for cx in range(dims[0]):
+        for cy in range(dims[1]):
+            x0 = 0.0 if cx == 0 else dx / 2 + 1e-9
+            x1 = lx if cx == dims[0] - 1 else lx - dx / 2 - 1e-9
+            y0 = 0.0 if cy == 0 else dy / 2 + 1e-9
+            y1 = ly if cy == dims[1] - 1 else ly - dy / 2 - 1e-9
+            x, y = rng.uniform(x0, x1, per_rank), rng.uniform(y0, y1, per_rank)
+            gx, gy = x + cx * (lx - dx), y + cy * (ly - dy)
+            rho = 1.0 + 0.1 * np.sin(3 * gx) * np.cos(2 * gy)
+            mu = np.exp(np.sin(2 * gx + gy))
+            out[(cx, cy)] = (x, y, rho, mu)
+    return out
+
+
+def _oracle_decomposed_steps(mk, dims, Nx, Ny, Lx, Ly, steps, iters):
+    """The decomposed timestep from oracle pieces: per-rank deposits + overlap sums + safeDivision, the solve
+    on the global grid (the decomposed iterate equals it), per-rank RK4 on the local slices, the exchange."""
+    nx_g, ny_g = domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)
+    dx, dy = Lx / (nx_g - 1), Ly / (ny_g - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    o = oracle.node_origins(dx, dy)
+    a = oracle.stokes_arrays(nx_g, ny_g)
+    ranks = {c: {n: oracle.zeros(Nx + s[0], Ny + s[1]) for n, s in (("rho_vy", (1, 0)), ("mu_b", (0, 0)), ("mu_p", (-1, -1)))}
+             for c in mk}
+    markers = {c: tuple(v.copy() for v in m) for c, m in mk.items()}
+    dt, dts = 0.0, []
+    for _ in range(steps):
+        for name, (xo, yo), q in (("rho_vy", ("x_rho", "y_rho"), 2), ("mu_b", ("x", "y"), 3), ("mu_p", ("x_p", "y_p"), 3)):
+            vws = {c: oracle.zeros(Nx + 1, Ny) for c in mk}
+            ws = {c: oracle.zeros(Nx + 1, Ny) for c in mk}
+            for c, m in markers.items():
+                oracle.bilinear_marker_to_grid(o[xo], o[yo], ranks[c][name], m[0], m[1], m[q], dx, dy, vws[c], ws[c])
+            oracle.sum_overlapping_values(ws, dims, Nx, Ny)
+            oracle.sum_overlapping_values(vws, dims, Nx, Ny)
+            for c in mk:
+                g = ranks[c][name]
+                nxv, nyv = g.shape
+                nz = ws[c][:nxv, :nyv] != 0
+                g[nz] = vws[c][:nxv, :nyv][nz] / ws[c][:nxv, :nyv][nz]
+                xs, ys = domains.local_slices(name, c, Nx, Ny)
+                a[name][xs, ys] = g
+        r = oracle.solve_stokes(a, 9.81, dx, dy, nx_g, ny_g, dt, 0.5, True, 1e-300, iters, 4)
+        dt = r.dt
+        dts.append(dt)
+        for c, m in markers.items():
+            xs, ys = domains.local_slices("Vx_pad", c, Nx, Ny)
+            vx = np.asfortranarray(a["Vx"][xs, ys])
+            xs, ys = domains.local_slices("Vy_pad", c, Nx, Ny)
+            vy = np.asfortranarray(a["Vy"][xs, ys])
+            oracle.move_markers_rk4(m[0], m[1], vx, vy, o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy, 1)
+        markers = oracle.exchange_markers(markers, dims, lx, ly, dx, dy)
+    return markers, a, dts
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims", [(2, 1), (2, 2)])
+def test_decomposed_timesteps_match_oracle(sf, dims):
+    Nx, Ny, Lx, Ly, steps, iters = 18, 14, 1.0, 0.8, 2, 600
+    nx_g, ny_g = domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)
+    dx, dy = Lx / (nx_g - 1), Ly / (ny_g - 1)
+    mk = _initial_markers(dims, Nx, Ny, dx, dy, 2500, 11)
+    st = domains.DecomposedStokesFlow2D(dims, Nx, Ny, Lx, Ly, {c: tuple(torch.from_numpy(v) for v in m) for c, m in mk.items()},
+                                        eps=1e-300, iter_max=iters)
+    dts = [st.step()["dt"] for _ in range(steps)]
+    ref_markers, ref_a, ref_dts = _oracle_decomposed_steps(mk, dims, Nx, Ny, Lx, Ly, steps, iters)
+    assert dts == ref_dts
+    vx, vy = st.velocities()
+    assert np.array_equal(vx.cpu().numpy(), ref_a["Vx"]) and np.array_equal(vy.cpu().numpy(), ref_a["Vy"])
+    for c in mk:
+        for q in range(4):
+            assert np.array_equal(st.markers[c][q].cpu().numpy(), ref_markers[c][q]), (c, q)
+    moved = sum(abs(len(ref_markers[c][0]) - len(mk[c][0])) for c in mk)
+    assert moved > 0          # markers did cross between ranks
