@@ -435,6 +435,19 @@ int sf_init_markers(sf_ctx* ctx, int64_t marker_density, double lx, double ly, d
                     double* x_m, double* y_m, void* stream);
 double sf_uniform(uint64_t seed, uint64_t counter);
 
+/* initializeMarkersCPU for the rank at (coord_x, coord_y) of a dims_x x
+ * dims_y grid (common.jl:40-90 with its boundary flags): sides shared with a
+ * neighbour leave the markers the neighbour places, so the ranks' markers tile
+ * the global domain.  Counts, then positions in local coordinates; the
+ * jitter as in sf_init_markers (its counter restarts on every rank).  With
+ * jitter and an odd density the reference then exchanges the markers
+ * (common.jl:94-96): call sf_exchange_markers. */
+int sf_marker_count_rank(int64_t marker_density, int64_t nx, int64_t ny, int32_t coord_x, int32_t coord_y,
+                         int32_t dims_x, int32_t dims_y, int64_t* nmx, int64_t* nmy);
+int sf_init_markers_rank(sf_ctx* ctx, int64_t marker_density, double lx, double ly, double dx, double dy,
+                         int64_t nx, int64_t ny, int32_t coord_x, int32_t coord_y, int32_t dims_x, int32_t dims_y,
+                         double jitter, uint64_t seed, double* x_m, double* y_m, void* stream);
+
 /* setInitialMarkerProperties! (common.jl:104-110) for the layered
  * air / plume / matrix model of StokesFlow2D_multixpu.jl:382-404:
  * y < air_height -> air, else (x-px)^2+(y-py)^2 < r^2 -> plume, else matrix. */

@@ -64,6 +64,9 @@ def lib():
         L.orc_uniform.restype = _d
         L.orc_marker_counts.argtypes = [_i64, _i64, _i64, _pi64, _pi64]
         L.orc_init_markers.argtypes = [_i64, _d, _d, _d, _d, _i64, _i64, _d, C.c_uint64, _pd, _pd]
+        L.orc_marker_counts_rank.argtypes = [_i64, _i64, _i64, C.c_int, C.c_int, C.c_int, C.c_int, _pi64, _pi64]
+        L.orc_init_markers_rank.argtypes = [_i64, _d, _d, _d, _d, _i64, _i64, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            _d, C.c_uint64, _pd, _pd]
         L.orc_set_marker_properties.argtypes = [C.POINTER(_PlumeModel), _pd, _pd, _i64, _d, _d, _pd, _pd]
         L.orc_bilinear_marker_to_grid.argtypes = [_d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d,
                                                   _pd, _pd, _i64, _i64, _pi64, _pi64]
@@ -118,6 +121,24 @@ def initialize_markers(marker_density, lx, ly, dx, dy, nx, ny, jitter=0.0, seed=
     x = np.empty(nmx * nmy)
     y = np.empty(nmx * nmy)
     lib().orc_init_markers(marker_density, lx, ly, dx, dy, nx, ny, jitter, seed, _p(x), _p(y))
+    return x, y
+
+
+def marker_counts_rank(marker_density, nx, ny, coords, dims):
+    """common.jl:43-66: markers in x / y on the rank at ``coords`` of a ``dims`` grid."""
+    a, b = _i64(), _i64()
+    lib().orc_marker_counts_rank(marker_density, nx, ny, coords[0], coords[1], dims[0], dims[1],
+                                 C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def initialize_markers_rank(marker_density, lx, ly, dx, dy, nx, ny, coords, dims, jitter=0.0, seed=0):
+    """common.jl:40-94 on the rank at ``coords``; lx, ly, nx, ny are the rank's local sizes."""
+    nmx, nmy = marker_counts_rank(marker_density, nx, ny, coords, dims)
+    x = np.empty(nmx * nmy)
+    y = np.empty(nmx * nmy)
+    lib().orc_init_markers_rank(marker_density, lx, ly, dx, dy, nx, ny, coords[0], coords[1], dims[0], dims[1],
+                                jitter, seed, _p(x), _p(y))
     return x, y
 
 

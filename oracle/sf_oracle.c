@@ -79,16 +79,38 @@ static double linrange_at(double a, double b, int64_t n, int64_t k) {
     return fma(t, b, fma(-t, a, a));
 }
 
-void orc_init_markers(int64_t marker_density, double lx, double ly, double dx, double dy,
-                      int64_t nx, int64_t ny, double jitter, uint64_t seed,
-                      double* x_m, double* y_m) {
+/* common.jl:43-67 for the rank at (cx, cy) of a dimx x dimy grid: limits and counts */
+static void rank_layout(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny, int cx,
+                        int cy, int dimx, int dimy, double* xlimlo, double* xlimhi, double* ylimlo, double* ylimhi,
+                        int64_t* nmx, int64_t* nmy) {
+    double dxm = dx / (double)md, dym = dy / (double)md;
+    int xlo = cx == 0, xhi = cx == dimx - 1, ylo = cy == 0, yhi = cy == dimy - 1;
+    double x_less_hi = md % 2 == 0 ? dxm / 2 : dxm, y_less_hi = md % 2 == 0 ? dym / 2 : dym;
+    double x_less_lo = md % 2 == 0 ? dxm / 2 : 0.0, y_less_lo = md % 2 == 0 ? dym / 2 : 0.0;
+    *xlimlo = xlo ? dxm / 2 : dx / 2 + x_less_lo;
+    *xlimhi = xhi ? lx - dxm / 2 : lx - dx / 2 - x_less_hi;
+    *ylimlo = ylo ? dym / 2 : dy / 2 + y_less_lo;
+    *ylimhi = yhi ? ly - dym / 2 : ly - dy / 2 - y_less_hi;
+    int64_t lo_less = md / 2, hi_less = (md + 1) / 2;   /* floor(md/2), ceil(md/2) */
+    *nmx = md * (nx - 1) - (xlo ? 0 : lo_less) - (xhi ? 0 : hi_less);
+    *nmy = md * (ny - 1) - (ylo ? 0 : lo_less) - (yhi ? 0 : hi_less);
+}
+
+void orc_marker_counts_rank(int64_t marker_density, int64_t nx, int64_t ny, int cx, int cy, int dimx, int dimy,
+                            int64_t* nmx, int64_t* nmy) {
+    double a, b, c, d;
+    rank_layout(marker_density, 1.0, 1.0, 1.0, 1.0, nx, ny, cx, cy, dimx, dimy, &a, &b, &c, &d, nmx, nmy);
+}
+
+void orc_init_markers_rank(int64_t marker_density, double lx, double ly, double dx, double dy, int64_t nx,
+                           int64_t ny, int cx, int cy, int dimx, int dimy, double jitter, uint64_t seed,
+                           double* x_m, double* y_m) {
     double dxm = dx / (double)marker_density;
     double dym = dy / (double)marker_density;
-    /* single rank: xlimlo = dxm/2, xlimhi = lx - dxm/2 (common.jl:65-68) */
-    double xlimlo = dxm / 2.0, xlimhi = lx - dxm / 2.0;
-    double ylimlo = dym / 2.0, ylimhi = ly - dym / 2.0;
+    double xlimlo, xlimhi, ylimlo, ylimhi;
     int64_t nmx, nmy;
-    orc_marker_counts(marker_density, nx, ny, &nmx, &nmy);
+    rank_layout(marker_density, lx, ly, dx, dy, nx, ny, cx, cy, dimx, dimy, &xlimlo, &xlimhi, &ylimlo, &ylimhi,
+                &nmx, &nmy);
     int64_t m = 0;
     for (int64_t ix = 1; ix <= nmx; ++ix) {       /* x outer, y inner (common.jl:85-91) */
         double xc = linrange_at(xlimlo, xlimhi, nmx, ix);
@@ -108,6 +130,13 @@ void orc_init_markers(int64_t marker_density, double lx, double ly, double dx, d
             y_m[k] = y_m[k] + (uy - 0.5) * jitter * dym;
         }
     }
+}
+
+void orc_init_markers(int64_t marker_density, double lx, double ly, double dx, double dy,
+                      int64_t nx, int64_t ny, double jitter, uint64_t seed,
+                      double* x_m, double* y_m) {
+    /* single rank: every boundary flag is true (common.jl:45-48 with dims = (1, 1)) */
+    orc_init_markers_rank(marker_density, lx, ly, dx, dy, nx, ny, 0, 0, 1, 1, jitter, seed, x_m, y_m);
 }
 
 /* StokesFlow2D_multixpu.jl:387-404 (density / viscosity closures) */

@@ -49,6 +49,18 @@ void orc_init_markers(int64_t marker_density, double lx, double ly, double dx, d
                       int64_t nx, int64_t ny, double jitter, uint64_t seed,
                       double* x_m, double* y_m);
 
+/* common.jl:40-90 for the rank at (cx, cy) of a dimx x dimy grid: the
+ * boundary flags (:45-48) move the limits inward by half a cell plus half a
+ * marker spacing on every side that faces a neighbour (:50-60) and drop
+ * floor(md/2) / ceil(md/2) marker columns there (:62-66).  lx, ly, nx, ny are
+ * the rank's local sizes.  The exchange that the reference runs after jitter
+ * with an odd density (:95-97) is not part of this function. */
+void orc_marker_counts_rank(int64_t marker_density, int64_t nx, int64_t ny, int cx, int cy, int dimx, int dimy,
+                            int64_t* nmx, int64_t* nmy);
+void orc_init_markers_rank(int64_t marker_density, double lx, double ly, double dx, double dy, int64_t nx,
+                           int64_t ny, int cx, int cy, int dimx, int dimy, double jitter, uint64_t seed,
+                           double* x_m, double* y_m);
+
 /* Material model used by the tests and the benchmark: a layered 'sticky air'
  * + circular plume + matrix model (StokesFlow2D_multixpu.jl:382-404 and the
  * test_StokesFlow2D.jl:208-230 variant).  kind 0 = density, 1 = viscosity. */

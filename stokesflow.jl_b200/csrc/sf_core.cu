@@ -177,18 +177,30 @@ struct MarkerLayout {
     int64_t nmx, nmy;
 };
 
-static MarkerLayout marker_layout(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny) {
+// the layout of the rank at (cx, cy) of a dims_x x dims_y grid (common.jl:43-75): a side that is a physical
+// boundary starts half a marker spacing in; a side shared with a neighbour leaves the markers the neighbour
+// places (half a cell, adjusted for odd or even densities)
+static MarkerLayout marker_layout_rank(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny,
+                                       int cx, int cy, int dimx, int dimy) {
     MarkerLayout L;
     L.dxm = dx / (double)md;
     L.dym = dy / (double)md;
-    // one rank: every side is a physical boundary (common.jl:54-57,65-68)
-    L.xlimlo = L.dxm / 2.0;
-    L.xlimhi = lx - L.dxm / 2.0;
-    L.ylimlo = L.dym / 2.0;
-    L.ylimhi = ly - L.dym / 2.0;
-    L.nmx = md * (nx - 1);   // common.jl:73-74
-    L.nmy = md * (ny - 1);
+    const bool xlo = cx == 0, xhi = cx == dimx - 1, ylo = cy == 0, yhi = cy == dimy - 1;   // :47-50
+    const bool even = md % 2 == 0;
+    const double x_less_hi = even ? L.dxm / 2 : L.dxm, y_less_hi = even ? L.dym / 2 : L.dym;   // :52-56
+    const double x_less_lo = even ? L.dxm / 2 : 0.0, y_less_lo = even ? L.dym / 2 : 0.0;
+    L.xlimlo = xlo ? L.dxm / 2 : dx / 2 + x_less_lo;                                          // :58-61
+    L.xlimhi = xhi ? lx - L.dxm / 2 : lx - dx / 2 - x_less_hi;
+    L.ylimlo = ylo ? L.dym / 2 : dy / 2 + y_less_lo;
+    L.ylimhi = yhi ? ly - L.dym / 2 : ly - dy / 2 - y_less_hi;
+    const int64_t lo_less = md / 2, hi_less = (md + 1) / 2;                                    // :63-64
+    L.nmx = md * (nx - 1) - (xlo ? 0 : lo_less) - (xhi ? 0 : hi_less);                         // :66-67
+    L.nmy = md * (ny - 1) - (ylo ? 0 : lo_less) - (yhi ? 0 : hi_less);
     return L;
+}
+
+static MarkerLayout marker_layout(int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny) {
+    return marker_layout_rank(md, lx, ly, dx, dy, nx, ny, 0, 0, 1, 1);   // one rank: every side is physical
 }
 
 // Julia LinRange(a, b, n)[k] (1-based k): lerpi(k-1, n-1, a, b) = fma(t, b, fma(-t, a, a))
@@ -379,6 +391,34 @@ int sf_init_markers(sf_ctx* c, int64_t md, double lx, double ly, double dx, doub
     MarkerLayout L = marker_layout(md, lx, ly, dx, dy, nx, ny);
     int64_t nm = L.nmx * L.nmy;
     if (nm == 0) return SF_OK;
+    unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nm, 256), (int64_t)c->num_sms * 16);
+    k_init_markers<<<blocks, 256, 0, as_stream(stream)>>>(L, jitter, seed, x, y);
+    SF_LAUNCHED(c);
+    return SF_OK;
+}
+
+int sf_marker_count_rank(int64_t md, int64_t nx, int64_t ny, int32_t coord_x, int32_t coord_y, int32_t dims_x,
+                         int32_t dims_y, int64_t* nmx, int64_t* nmy) {
+    if (md < 1 || nx < 3 || ny < 3 || !nmx || !nmy || dims_x < 1 || dims_y < 1 || coord_x < 0 || coord_x >= dims_x ||
+        coord_y < 0 || coord_y >= dims_y)
+        return fail(SF_ERR_INVALID_ARG, "sf_marker_count_rank: bad arguments");
+    MarkerLayout L = marker_layout_rank(md, 1.0, 1.0, 1.0, 1.0, nx, ny, coord_x, coord_y, dims_x, dims_y);
+    *nmx = L.nmx;
+    *nmy = L.nmy;
+    return SF_OK;
+}
+
+int sf_init_markers_rank(sf_ctx* c, int64_t md, double lx, double ly, double dx, double dy, int64_t nx, int64_t ny,
+                         int32_t coord_x, int32_t coord_y, int32_t dims_x, int32_t dims_y, double jitter,
+                         uint64_t seed, double* x, double* y, void* stream) {
+    if (!c || md < 1 || nx < 3 || ny < 3 || !x || !y || dims_x < 1 || dims_y < 1 || coord_x < 0 ||
+        coord_x >= dims_x || coord_y < 0 || coord_y >= dims_y)
+        return fail(SF_ERR_INVALID_ARG, "sf_init_markers_rank: bad arguments");
+    int rc = set_device(c);
+    if (rc) return rc;
+    MarkerLayout L = marker_layout_rank(md, lx, ly, dx, dy, nx, ny, coord_x, coord_y, dims_x, dims_y);
+    int64_t nm = L.nmx * L.nmy;
+    if (nm <= 0) return SF_OK;
     unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nm, 256), (int64_t)c->num_sms * 16);
     k_init_markers<<<blocks, 256, 0, as_stream(stream)>>>(L, jitter, seed, x, y);
     SF_LAUNCHED(c);

@@ -144,6 +144,9 @@ PROTOTYPES = {
     "sf_init_markers_host": (C.c_int, [_i64, _d, _d, _d, _d, _i64, _i64, _d, C.c_uint64, _vp, _vp]),
     "sf_init_markers": (C.c_int, [_vp, _i64, _d, _d, _d, _d, _i64, _i64, _d, C.c_uint64, _pd, _pd, _vp]),
     "sf_uniform": (_d, [C.c_uint64, C.c_uint64]),
+    "sf_marker_count_rank": (C.c_int, [_i64, _i64, _i64, _i32, _i32, _i32, _i32, C.POINTER(_i64), C.POINTER(_i64)]),
+    "sf_init_markers_rank": (C.c_int, [_vp, _i64, _d, _d, _d, _d, _i64, _i64, _i32, _i32, _i32, _i32, _d, C.c_uint64,
+                                       _pd, _pd, _vp]),
     "sf_set_marker_properties_host": (C.c_int, [C.POINTER(PlumeModelC), _vp, _vp, _i64, _d, _d, _vp, _vp]),
     "sf_set_marker_properties": (C.c_int, [_vp, C.POINTER(PlumeModelC), _pd, _pd, _i64, _d, _d, _pd, _pd, _vp]),
 }

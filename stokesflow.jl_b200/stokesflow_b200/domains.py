@@ -172,14 +172,71 @@ def exchange_markers(markers: dict, dims, lx, ly, dx, dy, contexts: dict) -> dic
     return {coord: tuple(t[:arr[k].n_out] for t in outs[coord]) for k, (coord, _) in enumerate(ranks)}
 
 
+def marker_count_rank(marker_density: int, Nx: int, Ny: int, coord, dims):
+    """Markers in x / y on the rank at ``coord`` (common.jl:43-66): a side that faces a neighbour loses
+    floor(md/2) (low side) or ceil(md/2) (high side) marker columns, so the ranks' markers tile the global
+    layout."""
+    a, b = C.c_int64(), C.c_int64()
+    check(lib().sf_marker_count_rank(int(marker_density), int(Nx), int(Ny), int(coord[0]), int(coord[1]),
+                                     int(dims[0]), int(dims[1]), C.byref(a), C.byref(b)), "marker_count_rank")
+    return a.value, b.value
+
+
+def rank_seed(seed: int, coord, dims) -> int:
+    """The jitter seed of a rank: ``seed`` plus its MPI rank in the Cartesian communicator (x slowest), so
+    that one rank draws what the one-domain ``initialize_markers`` draws with ``seed``."""
+    return int(seed) + coord[0] * dims[1] + coord[1]
+
+
+def initialize_markers_decomposed(dims, Nx: int, Ny: int, Lx: float, Ly: float, model, marker_density: int,
+                                  contexts: dict, *, jitter: float = 0.0, seed: int = 0) -> dict:
+    """initializeMarkersCPU then setInitialMarkerProperties! on every rank (StokesFlow2D_multixpu.jl:135-136,
+    common.jl:40-110), generated on each rank's device.  Each rank lays out its own part of the global marker
+    lattice in local coordinates; with jitter and an odd density the markers that jittered across a rank
+    boundary move to the neighbour through :func:`exchange_markers` with zero properties (common.jl:93-97),
+    and then the properties are set from the model at the global position ``x0 + x_m`` with
+    ``x0 = coord_x (Nx - 2) dx`` (StokesFlow2D_multixpu.jl:80-81).  ``model`` is an ``api.PlumeModel`` or any
+    object with ``marker_properties(x, y)``.  Returns {(cx, cy): (x_m, y_m, rho_m, mu_m)}."""
+    from . import api
+    dx = Lx / (global_size(dims[0], Nx) - 1)
+    dy = Ly / (global_size(dims[1], Ny) - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    out = {}
+    for coord, ctx in _ordered(contexts):
+        nmx, nmy = marker_count_rank(marker_density, Nx, Ny, coord, dims)
+        dev = f"cuda:{ctx.device}"
+        x = torch.empty(nmx * nmy, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        with torch.cuda.device(ctx.device):
+            check(lib().sf_init_markers_rank(ctx.handle, int(marker_density), float(lx), float(ly), float(dx),
+                                             float(dy), int(Nx), int(Ny), int(coord[0]), int(coord[1]),
+                                             int(dims[0]), int(dims[1]), float(jitter),
+                                             rank_seed(seed, coord, dims), x.data_ptr(), y.data_ptr(),
+                                             api._stream(None)), "initialize_markers_decomposed")
+        out[coord] = (x, y, torch.zeros_like(x), torch.zeros_like(x))
+    if jitter != 0.0 and marker_density % 2 == 1:
+        out = exchange_markers(out, dims, lx, ly, dx, dy, contexts)
+    for coord, (x, y, _, _) in out.items():
+        x0, y0 = coord[0] * (Nx - 2) * dx, coord[1] * (Ny - 2) * dy
+        with torch.cuda.device(contexts[coord].device):
+            if hasattr(model, "marker_properties"):
+                rho, mu = model.marker_properties(x0 + x, y0 + y)
+            else:
+                rho, mu = api.set_initial_marker_properties(x, y, model, x0, y0, ctx=contexts[coord])
+        out[coord] = (x, y, rho, mu)
+    return out
+
+
 class DecomposedStokesFlow2D:
     """The StokesFlow2D timestep loop (StokesFlow2D_multixpu.jl:157-191) on dims[0] x dims[1] ranks driven from
     this process: per timestep the three deposits with overlap sums, the decomposed solve, RK4 advection of
     each rank's markers on its local domain, and the marker exchange.  Nx, Ny: local grid points of a rank;
     Lx, Ly: the global domain.  markers {(cx, cy): (x_m, y_m, rho_m, mu_m)} in local coordinates (the ranks'
-    initial markers); devices {(cx, cy): CUDA device index} (default: the current device for all)."""
+    initial markers), or None to lay them out from ``model`` with :func:`initialize_markers_decomposed`;
+    devices {(cx, cy): CUDA device index} (default: the current device for all)."""
 
-    def __init__(self, dims, Nx: int, Ny: int, Lx: float, Ly: float, markers: dict, *, eps=1e-5, iter_max=100000,
+    def __init__(self, dims, Nx: int, Ny: int, Lx: float, Ly: float, markers: dict | None = None, *, model=None,
+                 marker_density: int = 4, jitter: float = 0.0, seed: int = 0, eps=1e-5, iter_max=100000,
                  g_y=9.81, maxdisp=0.5, devices: dict | None = None):
         from . import api
         from .driver import node_origins
@@ -199,6 +256,11 @@ class DecomposedStokesFlow2D:
                 z = lambda *s: api.zeros(*s, device=f"cuda:{dev}")  # noqa: E731
                 self.ranks[c] = {n: z(Nx + sx, Ny + sy) for n, (sx, sy) in ARRAYS.items()}
                 self.sums[c] = (z(Nx + 1, Ny), z(Nx + 1, Ny))   # interp_size (:112-114)
+        if markers is None:
+            if model is None:
+                raise ValueError("DecomposedStokesFlow2D: give markers or a model")
+            markers = initialize_markers_decomposed(dims, Nx, Ny, Lx, Ly, model, marker_density, self.ctx,
+                                                    jitter=jitter, seed=seed)
         self.markers = {c: tuple(t.to(f"cuda:{self.ranks[c]['P'].device.index}") for t in markers[c]) for c in coords}
 
     def step(self) -> dict:
