@@ -91,6 +91,10 @@ def parse():
     ap.add_argument("--serve-steps", default="1,20", help="timesteps per request, uniform range")
     ap.add_argument("--hbm-budget-gb", type=float, default=64.0)
     ap.add_argument("--fold-every", type=int, default=400)
+    ap.add_argument("--tile-rows", type=int, default=0,
+                    help="rows of the FP32 sweep tiles (8, 16, 32); 0: the autotuner chooses rows and schedule")
+    ap.add_argument("--tile-schedule", default=None, choices=["strided", "chunked"],
+                    help="schedule of the sweep tiles, with --tile-rows")
     return ap.parse_args()
 
 
@@ -422,7 +426,8 @@ def run_precision_form(a):
     rng = np.random.default_rng(a.seed)
     lo, hi = _pair(a.precision_contrast)
     md = sf.driver.marker_density_for(a.markers_per_cell)
-    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
+                            tile_schedule=a.tile_schedule)
     clocks = ClockSampler(0)
     clocks.start()
     cases = []
@@ -474,7 +479,8 @@ def run_batch_form(a):
     specs = workloads.batch_specs(a.batch_instances, a.seed, cells=_pair(a.batch_cells, int),
                                   mu_log10=_pair(a.mu_log10), mu_air=a.mu_air)
     inst = _deposit_instances(sf, specs)
-    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
+                            tile_schedule=a.tile_schedule)
 
     def mixed_problems(subset):
         probs, arrs = [], []
@@ -517,6 +523,7 @@ def run_batch_form(a):
     e1.record()
     torch.cuda.synchronize()
     mixed_s = e0.elapsed_time(e1) / 1e3
+    tiles = sf.batch_stats()   # the sweep shape used (the tuner's trial rounds are inside the timed region)
     e0.record()
     infos = [fp64_solve(d, s) for d, s in zip(inst[:k], fp64_arrs)]
     e1.record()
@@ -557,6 +564,9 @@ def run_batch_form(a):
                                          for f, v in errs.items()},
             "vs_tight_fp64": tight,
             "nonfinite_instances": [q for q, r in enumerate(res) if r["status"] == 5],
+            "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"], "tuner": tiles["tune_state"],
+                            "gpts_per_s_timed": {f"{r}/{c}": round(1.0 / v, 2) for (r, c), v in tiles["tune_ns"].items()
+                                                 if v > 0}},
             "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
             "clocks": clk,
             "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {a.batch_cells}, 9-25 "
@@ -576,7 +586,8 @@ def run_serve_form(a):
     kw = dict(cells=_pair(a.serve_cells, int), timesteps=_pair(a.serve_steps, int), mu_log10=_pair(a.mu_log10),
               mu_air=a.mu_air)
     budget = int(a.hbm_budget_gb * 2 ** 30)
-    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every)
+    opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
+                            tile_schedule=a.tile_schedule)
     # warm-up: one small request through each server
     for solver in ("mixed", "fp64"):
         w = serving.poisson_requests(1, 0.0, a.seed + 1, cells=(31, 31), timesteps=(1, 1))

@@ -306,7 +306,25 @@ typedef struct {
                                   inputs with dtau_local_max = 1 (its sweeps keep counting against
                                   max_sweeps); it converges on mixed soft/stiff layouts where the
                                   reference's step diverges.  Instances that converge are unaffected (1) */
+    int32_t tile_rows;         /* rows of the 32-column sweep tiles: 8, 16 or 32, or 0 to let the
+                                  autotuner choose the rows and the schedule.  The tuner times the first
+                                  rounds' sweeps in every shape and schedule (two rounds each), keeps the
+                                  fastest per point, and records it in the context for the workload class
+                                  (mean and total grid points), so later solves of that class start with
+                                  it.  Every shape and schedule computes the same bits, so the choice
+                                  changes the speed only (0)                                          */
+    int32_t tile_schedule;     /* with tile_rows set: 1 strided (CTA b of G takes tiles b, b+G, ...),
+                                  2 chunked (CTA b takes one contiguous run of tiles); 0 = 1.  With
+                                  tile_rows 0 it must be 0 (0)                                        */
 } sf_mixed_options;
+
+/* sf_engine_stats.tune_state */
+enum {
+    SF_TUNE_FIXED = 0,         /* the shape was given by tile_rows                        */
+    SF_TUNE_MEASURING = 1,     /* the tuner is still timing shapes                        */
+    SF_TUNE_MEASURED = 2,      /* the tuner chose the fastest shape it timed              */
+    SF_TUNE_CACHED = 3         /* the context held a measured shape for this workload     */
+};
 
 /* Solves n independent Stokes problems (each as in solveStokes!, with its own
  * grid size) to err <= eps by FP64 defect correction around FP32
@@ -354,6 +372,12 @@ typedef struct {
     int64_t sweeps;            /* FP32 sweep launches (one covers all instances) */
     int32_t active;            /* admitted, not finished                         */
     int32_t pending_results;   /* finished, not yet reported by sf_engine_step   */
+    int32_t tile_rows;         /* rows of the sweep tiles in use                 */
+    int32_t tile_schedule;     /* 1 strided, 2 chunked                           */
+    int32_t tune_state;        /* SF_TUNE_*                                      */
+    int32_t reserved;
+    double tune_ns[6];         /* best measured ns per point-sweep of 8 rows strided, 8 chunked, 16
+                                  strided, 16 chunked, 32 strided, 32 chunked (0: not timed) */
 } sf_engine_stats;
 
 /* Arena bytes one instance of Nx x Ny grid points holds while admitted. */
@@ -385,6 +409,11 @@ int sf_engine_step(sf_engine* e, void* stream, int64_t* finished, int32_t cap, i
                    int32_t* n_active);
 
 int sf_engine_get_stats(sf_engine* e, sf_engine_stats* stats);
+
+/* The stats of the engine that sf_solve_stokes_batch_mixed and
+ * sf_solve_stokes_mixed keep in the context, after their last call
+ * (SF_ERR_INVALID_ARG before the first). */
+int sf_ctx_batch_stats(sf_ctx* ctx, sf_engine_stats* stats);
 
 /* ---------------------------------------------------------------------- */
 /* RK4 marker advection and rebinning                                        */

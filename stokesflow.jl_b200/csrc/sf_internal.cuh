@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <cmath>
+#include <map>
 #include <string>
 
 #include "stokesflow_b200.h"
@@ -78,6 +79,8 @@ struct sf_ctx {
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_c = nullptr, ev_d = nullptr;
     int64_t launches = 0;         // kernels launched through this context
     sf_engine* batch_engine = nullptr;  // the engine sf_solve_stokes_batch_mixed reuses across calls
+    // sweep shapes the engines' autotuner measured best, by workload class (sf_mixed.cu)
+    std::map<int, int> sweep_shapes;
 };
 
 namespace sf {

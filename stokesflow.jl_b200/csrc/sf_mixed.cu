@@ -46,26 +46,28 @@
 namespace sf {
 namespace mx {
 
-#ifndef SF_PT32_BY
-#define SF_PT32_BY 16        // tile rows (a multiple of the 8 thread rows)
-#endif
-#ifndef SF_PT32_MINB
-#define SF_PT32_MINB 4       // CTAs per SM the register budget is sized for (56 KB of shared memory each)
-#endif
-constexpr int BX = 32, BY = SF_PT32_BY, TY = 8, RPT = BY / TY, NT = BX * TY;
-static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
-constexpr int TW = 36, TH = BY + 2;   // staged halo box; TW*4 bytes is a multiple of 16
-constexpr int W1 = BX + 1, H1 = BY + 1;
+// Sweep tiles are BX = 32 columns by BY rows, BY one of the shapes below (the autotuner picks it); 8 rows of
+// 32 threads, each thread BY/8 rows.  The FP64 kernels keep their own fixed 32 x 16 tiling, so the order of
+// their per-tile sums, and with it every residual and stopping decision, does not depend on the sweep shape.
+constexpr int BX = 32, TY = 8, NT = BX * TY;
+constexpr int BY64 = 16;              // tile rows of the FP64 kernels
+constexpr int TW = 36;                // staged halo box width; TW*4 bytes is a multiple of 16
+constexpr int W1 = BX + 1;
 constexpr int r128(int b) { return (b + 127) / 128 * 128; }
-constexpr int HALO_BYTES = r128(TH * TW * 4);
-constexpr int TILE_BYTES = r128(BY * BX * 4);
 constexpr int NHALO = 7;  // dVx, dVy, dP (current), mu_b, mu_p, rho, rdiv
 constexpr int NTILE = 4;  // rate_x, rate_y, rx, ry
-constexpr int STAGE_BYTES = NHALO * HALO_BYTES + NTILE * TILE_BYTES;
-constexpr uint32_t STAGE_TX = NHALO * TH * TW * 4 + NTILE * BY * BX * 4;
-constexpr int ST1_BYTES = r128(H1 * W1 * 4);
 constexpr int NST = 2;
-constexpr int SMEM_BYTES = NST * STAGE_BYTES + ST1_BYTES + 64;   // + tau_xy (the others live in the stage)
+template <int BY>
+struct Shape {
+    static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
+    static constexpr int TH = BY + 2, H1 = BY + 1, RPT = BY / TY;
+    static constexpr int HALO_BYTES = r128(TH * TW * 4);
+    static constexpr int TILE_BYTES = r128(BY * BX * 4);
+    static constexpr int STAGE_BYTES = NHALO * HALO_BYTES + NTILE * TILE_BYTES;
+    static constexpr uint32_t STAGE_TX = NHALO * TH * TW * 4 + NTILE * BY * BX * 4;
+    static constexpr int ST1_BYTES = r128(H1 * W1 * 4);
+    static constexpr int SMEM_BYTES = NST * STAGE_BYTES + ST1_BYTES + 64;   // + tau_xy (the others live in the stage)
+};
 constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;
 
 // FP32 fields of an instance (each LD32 x rows floats)
@@ -76,7 +78,8 @@ enum { D_VX, D_VY, D_P, D_RHO, D_MUB, D_MUP, D_NUM };
 enum { M_VXA, M_VXB, M_VYA, M_VYB, M_PA, M_PB, M_MUB, M_MUP, M_RHO, M_RDIV, M_RVX, M_RVY, M_RX, M_RY, M_NUM };
 
 struct Inst {  // device-side description of one instance
-    int Nx, Ny, ntx, nty;
+    int Nx, Ny;
+    int ntx, pad_;          // tiles in x (32 columns for the sweeps and the FP64 kernels alike, whatever the rows)
     int64_t LD32, LD64, rows;
     float* f32;             // G_NUM fields
     double* f64;            // D_NUM fields
@@ -95,9 +98,17 @@ __device__ __forceinline__ double* gd(const Inst& I, int k) { return I.f64 + (in
 // ---------------------------------------------------------------------------
 // FP32 PT sweep over a tile work list (tiles: {instance, tile index})
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __restrict__ maps, const Inst* __restrict__ insts,
-                                               const int2* __restrict__ tiles, const int* __restrict__ ntiles_ptr,
-                                               int launch_parity, int* __restrict__ err_flag) {
+// The arithmetic of a point does not depend on BY: the file is compiled without contraction and the fused
+// multiply-adds below are written out, so every shape (and a change of shape between sweeps) gives the same bits.
+template <int BY, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict__ maps, const Inst* __restrict__ insts,
+                                                   const int2* __restrict__ tiles, const int* __restrict__ ntiles_ptr,
+                                                   int launch_parity, int chunked, int* __restrict__ err_flag) {
+    using S = Shape<BY>;
+    constexpr int TH = S::TH, H1 = S::H1, RPT = S::RPT, HALO_BYTES = S::HALO_BYTES, TILE_BYTES = S::TILE_BYTES;
+    constexpr int STAGE_BYTES = S::STAGE_BYTES, ST1_BYTES = S::ST1_BYTES;
+    constexpr uint32_t STAGE_TX = S::STAGE_TX;
+    (void)TH;
     extern __shared__ __align__(128) unsigned char smem[];
     typedef float Row1[W1];
     typedef float RowH[TW];
@@ -112,12 +123,22 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         fence_mbar_init();
     }
     __syncthreads();
+    // the tile list is ordered by instance, so a CTA meets each instance in one run of tiles: the maps it
+    // reads are fenced when the run starts
+    int fenced = -1;
     auto issue = [&](int t, int s) {  // thread 0 only
         const int2 td = tiles[t];
         const Inst& I = insts[td.x];
         const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
         const int in = (I.parity ^ launch_parity) & 1;
         const CUtensorMap* M = maps + (int64_t)td.x * M_NUM;
+        if (td.x != fenced) {
+            fence_tensormap_acquire(&M[in ? M_VXB : M_VXA]);
+            fence_tensormap_acquire(&M[in ? M_VYB : M_VYA]);
+            fence_tensormap_acquire(&M[in ? M_PB : M_PA]);
+            for (int m = M_MUB; m < M_NUM; ++m) fence_tensormap_acquire(&M[m]);
+            fenced = td.x;
+        }
         unsigned char* st = smem + s * STAGE_BYTES;
         mbar_arrive_expect_tx(&bar[s], STAGE_TX);
         tma_load_2d(st + 0 * HALO_BYTES, &M[in ? M_VXB : M_VXA], &bar[s], i0, j0);
@@ -133,11 +154,24 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         tma_load_2d(tb + 2 * TILE_BYTES, &M[M_RX], &bar[s], i0, j0);
         tma_load_2d(tb + 3 * TILE_BYTES, &M[M_RY], &bar[s], i0, j0);
     };
+    // schedule: strided (CTA b takes tiles b, b + G, ...: neighbouring tiles run side by side) or chunked (CTA b
+    // takes a contiguous run of ceil(ntiles / G) tiles: it meets few instances, so it fences few maps)
     const int G = gridDim.x;
-    int t = blockIdx.x;
+    int first, step, end;
+    if (chunked) {
+        const int chunk = (ntiles + G - 1) / G;
+        first = blockIdx.x * chunk;
+        step = 1;
+        end = min(ntiles, first + chunk);
+    } else {
+        first = blockIdx.x;
+        step = G;
+        end = ntiles;
+    }
+    int t = first;
     if (tid == 0)
         for (int k = 0; k < NST - 1; ++k)
-            if (t + k * G < ntiles) issue(t + k * G, k);
+            if (t + k * step < end) issue(t + k * step, k);
     uint32_t phase = 0;
     int s = 0;
     // a copy never completed: flag it, give every copy still in flight a bounded chance to land (the issuing
@@ -146,7 +180,7 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         if (tid == 0) {
             atomicExch(err_flag, 1);
             for (int k = 0; k < NST; ++k) {
-                if (t + k * G >= ntiles) break;
+                if (t + k * step >= end) break;
                 const int sk = (s + k) % NST;
                 const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
                 mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
@@ -154,9 +188,9 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         }
         __syncthreads();
     };
-    for (; t < ntiles; t += G) {
-        const int tn = t + (NST - 1) * G;
-        if (tid == 0 && tn < ntiles) issue(tn, (s + NST - 1) % NST);
+    for (; t < end; t += step) {
+        const int tn = t + (NST - 1) * step;
+        if (tid == 0 && tn < end) issue(tn, (s + NST - 1) % NST);
         // the timeout vote rides on the stage-1 barrier below: stage 1 writes shared memory only, so a thread
         // whose copy did not land computes garbage there and nothing else before everyone leaves
         const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
@@ -190,6 +224,7 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         float* Rvx = gf(I, G_RVX) + tbase;
         float* Rvy = gf(I, G_RVY) + tbase;
         const float c_pt = I.c_ptscf, dampX = I.dampXf, dampY = I.dampYf, g_dt = I.g_dtf;
+        const float h_dx = 0.5f * _dx, h_dy = 0.5f * _dy;
         // pseudo-time step c_vsc / mu_av = (2 c_vsc) / (mu_0 + mu_1) (the reference's average, :129-130), or
         // c_vsc / (largest viscosity of the node's stencil); the FP32 sweeps only drive the correction, so the
         // fast division is enough
@@ -212,9 +247,10 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
                 float div_d = dVx_dx + dVy_dy;
                 float div_full = div_d + sRdiv[b][a];          // divV of V_k + dV
                 float mu = sMup[b][a];
-                float pn = sPo[b][a] - c_pt * mu * div_full;
-                sSxx[b][a] = 2.0f * mu * (dVx_dx - (1.0f / 3.0f) * div_d) - pn;
-                sSyy[b][a] = 2.0f * mu * (dVy_dy - (1.0f / 3.0f) * div_d) - pn;
+                float pn = fmaf(-(c_pt * mu), div_full, sPo[b][a]);
+                float mu2 = 2.0f * mu;
+                sSxx[b][a] = fmaf(mu2, fmaf(-(1.0f / 3.0f), div_d, dVx_dx), -pn);
+                sSyy[b][a] = fmaf(mu2, fmaf(-(1.0f / 3.0f), div_d, dVy_dy), -pn);
                 if (a < BX && b < BY) P_out[a + b * ldi] = pn;
             }
             if (interior || (i < Nx && j < Ny)) {
@@ -234,26 +270,27 @@ __global__ void __launch_bounds__(NT, SF_PT32_MINB) k_pt32(const CUtensorMap* __
         }
         // ---- stage 2: damped rates and velocity update of the correction ----
         auto rate_x = [&](int a, int b, int o) {
-            float Rx = (sSxx[b][a + 1] - sSxx[b][a]) * _dx + (sTxy[b + 1][a + 1] - sTxy[b][a + 1]) * _dy + sRx[b][a];
-            float dv = dampX * sRvx[b][a] + Rx;
+            float Rx = fmaf(sSxx[b][a + 1] - sSxx[b][a], _dx, fmaf(sTxy[b + 1][a + 1] - sTxy[b][a + 1], _dy, sRx[b][a]));
+            float dv = fmaf(dampX, sRvx[b][a], Rx);
             Rvx[o] = dv;
             float dtau = dmax ? __fdividef(c_vsc, fmaxf(fmaxf(sMup[b][a], sMup[b][a + 1]),
                                                        fmaxf(sMub[b][a + 1], sMub[b + 1][a + 1])))
                               : __fdividef(c_vsc2, sMup[b][a] + sMup[b][a + 1]);
-            return sVx[b + 1][a + 1] + dtau * dv;
+            return fmaf(dtau, dv, sVx[b + 1][a + 1]);
         };
         auto rate_y = [&](int a, int b, int o) {
             float av = 0.25f * (sVx[b + 1][a] + sVx[b + 1][a + 1] + sVx[b + 2][a] + sVx[b + 2][a + 1]);
             float dxr = sRho[b + 1][a + 2] - sRho[b + 1][a];
             float dyr = sRho[b + 2][a + 1] - sRho[b][a + 1];
-            float Ry = (sSyy[b + 1][a] - sSyy[b][a]) * _dy + (sTxy[b + 1][a + 1] - sTxy[b + 1][a]) * _dx -
-                       g_dt * (av * dxr * 0.5f * _dx + sVy[b + 1][a + 1] * dyr * 0.5f * _dy) + sRy[b][a];
-            float dv = dampY * sRvy[b][a] + Ry;
+            float stab = fmaf(av * dxr, h_dx, (sVy[b + 1][a + 1] * dyr) * h_dy);
+            float Ry = fmaf(sSyy[b + 1][a] - sSyy[b][a], _dy,
+                            fmaf(sTxy[b + 1][a + 1] - sTxy[b + 1][a], _dx, fmaf(-g_dt, stab, sRy[b][a])));
+            float dv = fmaf(dampY, sRvy[b][a], Ry);
             Rvy[o] = dv;
             float dtau = dmax ? __fdividef(c_vsc, fmaxf(fmaxf(sMup[b][a], sMup[b + 1][a]),
                                                        fmaxf(sMub[b + 1][a], sMub[b + 1][a + 1])))
                               : __fdividef(c_vsc2, sMup[b][a] + sMup[b + 1][a]);
-            return sVy[b + 1][a + 1] + dtau * dv;
+            return fmaf(dtau, dv, sVy[b + 1][a + 1]);
         };
         if (interior) {
 #pragma unroll
@@ -338,11 +375,11 @@ __global__ void __launch_bounds__(T64) k_maxv64(const Inst* __restrict__ insts, 
     __shared__ double sh[T64 / 32];
     const int2 td = tiles[blockIdx.x];
     const Inst& I = insts[td.x];
-    const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
+    const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY64;
     const double* Vx = gd(I, D_VX);
     const double* Vy = gd(I, D_VY);
     double mx = 0.0, my = 0.0;
-    for (int k = threadIdx.x; k < BX * BY; k += T64) {
+    for (int k = threadIdx.x; k < BX * BY64; k += T64) {
         const int i = i0 + (k % BX), j = j0 + (k / BX);
         if (i < I.Nx - 2 && j < I.Ny - 1) mx = fmax(mx, fabs(Vx[(i + 1) + (int64_t)(j + 1) * I.LD64]));
         if (i < I.Nx - 1 && j < I.Ny - 2) my = fmax(my, fabs(Vy[(i + 1) + (int64_t)(j + 1) * I.LD64]));
@@ -362,7 +399,7 @@ __global__ void __launch_bounds__(T64) k_resid64(const Inst* __restrict__ insts,
     const int2 td = tiles[blockIdx.x];
     const Inst& I = insts[td.x];
     const int Nx = I.Nx, Ny = I.Ny;
-    const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
+    const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY64;
     const int64_t L = I.LD64, L32 = I.LD32;
     const double* Vx = gd(I, D_VX);
     const double* Vy = gd(I, D_VY);
@@ -389,7 +426,7 @@ __global__ void __launch_bounds__(T64) k_resid64(const Inst* __restrict__ insts,
         return 2.0 * mub[i + (int64_t)j * L] * 0.5 * (dVx_dy + dVy_dx);
     };
     double srx = 0.0, sry = 0.0, sdv = 0.0;
-    for (int k = threadIdx.x; k < BX * BY; k += T64) {
+    for (int k = threadIdx.x; k < BX * BY64; k += T64) {
         const int i = i0 + (k % BX), j = j0 + (k / BX);
         if (i >= Nx - 1 || j >= Ny - 1) continue;
         const int64_t o = i + (int64_t)j * L, o32 = i + (int64_t)j * L32;
@@ -570,6 +607,50 @@ namespace mx {
 
 static unsigned grid1(int64_t n, int per) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + per - 1) / per, 65535)); }
 
+// The sweep shapes the autotuner chooses from: tile rows, and the CTAs per SM that the register budget is
+// sized for (the shared memory of a CTA grows with the rows: 31, 56 and 105 KB).
+typedef void (*SweepKernel)(const CUtensorMap*, const Inst*, const int2*, const int*, int, int, int*);
+struct SweepShape {
+    int rows, minb, smem;
+    SweepKernel kern;
+};
+static const SweepShape kShapes[] = {
+    {8, 4, Shape<8>::SMEM_BYTES, k_pt32<8, 4>},
+    {16, 4, Shape<16>::SMEM_BYTES, k_pt32<16, 4>},
+    {32, 2, Shape<32>::SMEM_BYTES, k_pt32<32, 2>},
+};
+constexpr int NSHAPES = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
+// tile schedules of the persistent sweep kernel: 0 strided, 1 chunked (the kernel's `chunked` argument)
+constexpr int NSCHED = 2;
+// the tuner's candidates: shape k with schedule c is candidate k * NSCHED + c
+constexpr int NCAND = NSHAPES * NSCHED;
+static_assert(NCAND == 6, "sf_engine_stats.tune_ns has one entry per candidate");
+constexpr int DEFAULT_SHAPE = 1;                      // 32 x 16 rows ...
+constexpr int DEFAULT_CAND = DEFAULT_SHAPE * NSCHED + 1;  // ... chunked, until measured otherwise
+constexpr int TUNE_PASSES = 2;                        // timed pieces per candidate; the fastest counts
+
+static int shape_of_rows(int rows) {
+    for (int k = 0; k < NSHAPES; ++k)
+        if (kShapes[k].rows == rows) return k;
+    return -1;
+}
+
+// resident CTAs per SM of each shape on a device (0: not yet queried); the attribute is set per device
+static int shape_per_sm(int device, int k, int* out) {
+    static int cache[64][NSHAPES] = {};
+    if (device < 0 || device >= 64) return fail(SF_ERR_INVALID_ARG, "sf_engine: device index");
+    if (!cache[device][k]) {
+        const SweepShape& sh = kShapes[k];
+        SF_CUDA(cudaFuncSetAttribute((const void*)sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem));
+        int n = 0;
+        SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, (const void*)sh.kern, NT, sh.smem));
+        if (n < 1) return fail(SF_ERR_CUDA, "k_pt32 does not fit on an SM");
+        cache[device][k] = n;
+    }
+    *out = cache[device][k];
+    return SF_OK;
+}
+
 // arena bytes of one instance: FP32 fields, then FP64 fields, each 256-byte aligned
 struct Layout {
     int64_t LD, rows, fstride, bytes32, bytes64;
@@ -633,7 +714,9 @@ struct Slot {  // an admitted instance
     sf_batch_instance* user = nullptr;
     int64_t ticket = -1;
     Inst d;                    // source of the device record
-    int64_t ntiles = 0, off = 0, bytes = 0;
+    int64_t ntiles[NSHAPES] = {};  // sweep tiles in each shape
+    int64_t ntiles64 = 0;      // FP64-kernel tiles
+    int64_t off = 0, bytes = 0;
     bool active = false;
     bool swept = false;        // ran sweeps since its last fold
     int64_t inner_total = 0, outer = 0;
@@ -651,6 +734,8 @@ static sf_mixed_options normalized(const sf_mixed_options* o) {
         r.use_graphs = 1;
         r.dtau_local_max = 0;
         r.retry_local_max = 1;
+        r.tile_rows = 0;
+        r.tile_schedule = 0;
     }
     if (r.fold_every < 2) r.fold_every = 2;
     r.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
@@ -675,31 +760,48 @@ struct sf_engine {
     // device tables, one allocation: insts | maps | segs | out | scale | list | ntiles | flag
     void* tables = nullptr;
     Inst* d_insts = nullptr;
-    CUtensorMap* d_maps = nullptr;
+    CUtensorMap* d_maps = nullptr;       // [shape][slot][M_NUM]: every slot's maps for every shape
     Seg* d_segs = nullptr;
     double* d_out = nullptr;
     double* d_scale = nullptr;
     int* d_list = nullptr;
-    int* d_ntiles = nullptr;
+    int* d_ntiles = nullptr;             // [shape]
     int* d_flag = nullptr;               // a bounded wait of k_pt32 gave up
     double* h_out = nullptr;             // pinned mirror of d_out
-    // tile list and per-tile partials, grown on demand
-    int2* d_tiles = nullptr;
+    // the sweep tile list (current shape), and the FP64-kernel tile list with its per-tile partials; grown on demand
+    int2* d_tiles[NSHAPES] = {};         // one sweep list per shape (tile counts differ)
+    int64_t tile_cap[NSHAPES] = {};
+    int2* d_tiles64 = nullptr;
     double* d_part = nullptr;
-    int64_t tile_cap = 0;
+    int64_t tile64_cap = 0;
     std::vector<int2> h_tiles;
     std::vector<Seg> h_segs;
-    int h_ntiles = 0;                    // source of the tile-count upload
+    int h_ntiles[NSHAPES] = {};          // sources of the tile-count uploads
+    std::vector<int2> h_list[NSHAPES];   // sources of the sweep-list uploads
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     int graph_k = 0;
-    int blocks = 0;
+    int blocks = 0;                      // persistent CTAs of the current shape
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    // sweep shape and its autotuner: while measuring, each round's sweeps run in the next shape to try and are
+    // timed on the engine stream; the shape with the fewest ns per point-sweep is kept and recorded in the context
+    int shape = DEFAULT_SHAPE;
+    int sched = 0;
+    int tune_state = SF_TUNE_MEASURING;
+    int tune_trials = 0;
+    int tune_key = -1;
+    double tune_ns[NCAND] = {};          // best ns per point-sweep of each candidate (0: not measured)
+    int timed_first = 0;                 // the last round timed trials timed_first ...
+    int timed_pieces = 0;                // ... up to timed_first + timed_pieces - 1 (candidate = trial % NCAND),
+    double timed_points = 0.0;           // each piece over this many point-sweeps
+    cudaEvent_t ev_piece[NCAND * TUNE_PASSES + 1] = {};
     int64_t next_ticket = 0, submitted = 0, finished = 0, rounds = 0, sweeps = 0;
     std::deque<int64_t> pending;
 };
 
 namespace {
+
+CUtensorMap* maps_of(sf_engine* e, int k) { return e->d_maps + (size_t)k * e->slots.size() * M_NUM; }
 
 void drop_graph(sf_engine* e) {
     if (e->gexec) cudaGraphExecDestroy(e->gexec);
@@ -713,15 +815,21 @@ void engine_free(sf_engine* e) {
     if (e->s) cudaStreamSynchronize(e->s);
     drop_graph(e);
     if (e->tables) cudaFree(e->tables);
-    if (e->d_tiles) cudaFree(e->d_tiles);
+    for (int2* t : e->d_tiles)
+        if (t) cudaFree(t);
+    if (e->d_tiles64) cudaFree(e->d_tiles64);
     if (e->d_part) cudaFree(e->d_part);
     if (e->h_out) cudaFreeHost(e->h_out);
     if (e->arena_owned && e->arena) cudaFree(e->arena);
     if (e->ev_in) cudaEventDestroy(e->ev_in);
     if (e->ev_out) cudaEventDestroy(e->ev_out);
+    for (cudaEvent_t ev : e->ev_piece)
+        if (ev) cudaEventDestroy(ev);
     if (e->s) cudaStreamDestroy(e->s);
     delete e;
 }
+
+int configure_tuner(sf_engine* e);
 
 int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options* o) {
     e->ctx = ctx;
@@ -729,9 +837,10 @@ int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options*
     SF_CUDA(cudaStreamCreateWithFlags(&e->s, cudaStreamNonBlocking));
     SF_CUDA(cudaEventCreateWithFlags(&e->ev_in, cudaEventDisableTiming));
     SF_CUDA(cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming));
+    for (cudaEvent_t& ev : e->ev_piece) SF_CUDA(cudaEventCreate(&ev));
     const size_t n = (size_t)slot_cap;
     const size_t o_ins = 0, o_map = round_up(o_ins + n * sizeof(Inst), 256);
-    const size_t o_seg = round_up(o_map + n * M_NUM * sizeof(CUtensorMap), 256);
+    const size_t o_seg = round_up(o_map + (size_t)NSHAPES * n * M_NUM * sizeof(CUtensorMap), 256);
     const size_t o_out = round_up(o_seg + n * sizeof(Seg), 256);
     const size_t o_scl = round_up(o_out + n * 3 * 8, 256);
     const size_t o_lst = round_up(o_scl + n * 8, 256);
@@ -756,74 +865,224 @@ int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options*
     e->slots.assign(n, Slot{});
     e->free_slots.clear();
     for (int k = slot_cap - 1; k >= 0; --k) e->free_slots.push_back(k);
-    static int per_sm = 0;
-    if (!per_sm) {
-        SF_CUDA(cudaFuncSetAttribute(k_pt32, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        SF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pt32, NT, SMEM_BYTES));
-        if (per_sm < 1) return fail(SF_ERR_CUDA, "k_pt32 does not fit on an SM");
-    }
-    e->blocks = per_sm * ctx->num_sms;  // persistent: one wave; CTAs beyond the tile count exit at once
-    return SF_OK;
+    return configure_tuner(e);
 }
 
-int ensure_tiles(sf_engine* e, int64_t need) {
-    if (need <= e->tile_cap) return SF_OK;
-    const int64_t cap = std::max<int64_t>({need, 2 * e->tile_cap, 4096});
-    SF_CUDA(cudaStreamSynchronize(e->s));  // the old lists may still be read by queued sweeps
-    drop_graph(e);                         // the graph holds the old pointer
-    if (e->d_tiles) cudaFree(e->d_tiles);
-    if (e->d_part) cudaFree(e->d_part);
-    e->d_tiles = nullptr;
-    e->d_part = nullptr;
-    e->tile_cap = 0;
-    if (cudaMalloc(&e->d_tiles, (size_t)cap * sizeof(int2)) != cudaSuccess ||
-        cudaMalloc(&e->d_part, (size_t)cap * 3 * 8) != cudaSuccess) {
+// grows a device tile list (and, for the FP64 list, its per-tile partials)
+int grow_list(sf_engine* e, int64_t need, int2** tiles, double** part, int64_t* cap_io) {
+    if (need <= *cap_io) return SF_OK;
+    const int64_t cap = std::max<int64_t>({need, 2 * *cap_io, 4096});
+    SF_CUDA(cudaStreamSynchronize(e->s));  // the old list may still be read by queued kernels
+    if (*tiles) cudaFree(*tiles);
+    if (part && *part) cudaFree(*part);
+    *tiles = nullptr;
+    if (part) *part = nullptr;
+    *cap_io = 0;
+    if (cudaMalloc(tiles, (size_t)cap * sizeof(int2)) != cudaSuccess ||
+        (part && cudaMalloc(part, (size_t)cap * 3 * 8) != cudaSuccess)) {
         cudaGetLastError();
         return fail(SF_ERR_OOM, "sf_engine: tile list");
     }
-    e->tile_cap = cap;
-    e->h_tiles.resize((size_t)cap);
+    *cap_io = cap;
+    if ((int64_t)e->h_tiles.size() < cap) e->h_tiles.resize((size_t)cap);
     return SF_OK;
 }
 
-// tile list + segments of the slots in `ids` -> device; returns the tile count in *nt
-int upload_lists(sf_engine* e, const std::vector<int>& ids, bool segs, int64_t* nt_out) {
+// FP64-kernel tile list + segments of the slots in `ids` -> device; returns the tile count in *nt_out
+int upload_lists64(sf_engine* e, const std::vector<int>& ids, int64_t* nt_out) {
     int64_t nt = 0;
-    for (int q : ids) nt += e->slots[q].ntiles;
-    int rc = ensure_tiles(e, nt);
+    for (int q : ids) nt += e->slots[q].ntiles64;
+    int rc = grow_list(e, nt, &e->d_tiles64, &e->d_part, &e->tile64_cap);
     if (rc) return rc;
-    if (segs) e->h_segs.resize(ids.size());
+    e->h_segs.resize(ids.size());
     int64_t k = 0;
     for (size_t q = 0; q < ids.size(); ++q) {
         const Slot& h = e->slots[ids[q]];
-        if (segs) e->h_segs[q] = Seg{ids[q], (int)k, (int)(k + h.ntiles), 0};
-        for (int64_t t = 0; t < h.ntiles; ++t) e->h_tiles[k++] = make_int2(ids[q], (int)t);
+        e->h_segs[q] = Seg{ids[q], (int)k, (int)(k + h.ntiles64), 0};
+        for (int64_t t = 0; t < h.ntiles64; ++t) e->h_tiles[k++] = make_int2(ids[q], (int)t);
     }
     // pageable sources: the copies are staged before cudaMemcpyAsync returns, so the host vectors are free again
-    SF_CUDA(cudaMemcpyAsync(e->d_tiles, e->h_tiles.data(), (size_t)nt * sizeof(int2), cudaMemcpyHostToDevice, e->s));
-    if (segs)
-        SF_CUDA(cudaMemcpyAsync(e->d_segs, e->h_segs.data(), ids.size() * sizeof(Seg), cudaMemcpyHostToDevice, e->s));
-    e->h_ntiles = (int)nt;
-    SF_CUDA(cudaMemcpyAsync(e->d_ntiles, &e->h_ntiles, sizeof(int), cudaMemcpyHostToDevice, e->s));
+    SF_CUDA(cudaMemcpyAsync(e->d_tiles64, e->h_tiles.data(), (size_t)nt * sizeof(int2), cudaMemcpyHostToDevice, e->s));
+    SF_CUDA(cudaMemcpyAsync(e->d_segs, e->h_segs.data(), ids.size() * sizeof(Seg), cudaMemcpyHostToDevice, e->s));
     *nt_out = nt;
     return SF_OK;
 }
 
-int launch_sweeps(sf_engine* e) {
-    const int K = e->opt.fold_every;
-    auto run = [&]() -> int {
-        for (int k = 0; k < K; ++k) {
-            k_pt32<<<e->blocks, dim3(BX, TY), SMEM_BYTES, e->s>>>(e->d_maps, e->d_insts, e->d_tiles, e->d_ntiles,
-                                                                   k & 1, e->d_flag);
-            SF_CHECK_LAUNCH();
+// sweep tile list of the slots in `ids` for shape k, and its length -> device
+int upload_sweep_list(sf_engine* e, const std::vector<int>& ids, int k) {
+    int64_t nt = 0;
+    for (int q : ids) nt += e->slots[q].ntiles[k];
+    if (nt > e->tile_cap[k]) drop_graph(e);  // the graph may hold the old pointer
+    int rc = grow_list(e, nt, &e->d_tiles[k], nullptr, &e->tile_cap[k]);
+    if (rc) return rc;
+    std::vector<int2>& h = e->h_list[k];
+    h.resize((size_t)nt);
+    int64_t n = 0;
+    for (int q : ids)
+        for (int64_t t = 0; t < e->slots[q].ntiles[k]; ++t) h[(size_t)n++] = make_int2(q, (int)t);
+    SF_CUDA(cudaMemcpyAsync(e->d_tiles[k], h.data(), (size_t)nt * sizeof(int2), cudaMemcpyHostToDevice, e->s));
+    e->h_ntiles[k] = (int)nt;
+    SF_CUDA(cudaMemcpyAsync(e->d_ntiles + k, &e->h_ntiles[k], sizeof(int), cudaMemcpyHostToDevice, e->s));
+    return SF_OK;
+}
+
+// sweep tilings of slot q: its tile count and its 14 tensor maps (box = tile + halo, or tile) in every shape,
+// encoded once at admission, so that a change of shape is a choice of pointers
+int encode_maps(sf_engine* e, int q) {
+    Slot& h = e->slots[q];
+    const Inst& I = h.d;
+    const int gmap[M_NUM] = {G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_MUB, G_MUP, G_RHO, G_RDIV,
+                             G_RVX, G_RVY, G_RX, G_RY};
+    CUtensorMap maps[M_NUM];
+    for (int k = 0; k < NSHAPES; ++k) {
+        const int rows = kShapes[k].rows;
+        h.ntiles[k] = (int64_t)I.ntx * ceil_div(I.Ny - 1, rows);
+        for (int m = 0; m < M_NUM; ++m) {
+            const bool halo = m <= M_RDIV;
+            int rc = encode_tmap_f32(&maps[m], I.f32 + (int64_t)gmap[m] * I.fstride32, I.LD32, I.rows,
+                                     halo ? TW : BX, halo ? rows + 2 : rows);
+            if (rc) return rc;
         }
-        return SF_OK;
-    };
+        // pageable source: staged before the call returns, so `maps` is free again
+        SF_CUDA(cudaMemcpyAsync(maps_of(e, k) + (size_t)q * M_NUM, maps, sizeof(maps), cudaMemcpyHostToDevice, e->s));
+    }
+    return SF_OK;
+}
+
+// switches the sweeps to shape k with schedule c (persistent grid size; the maps and lists are per shape)
+int use_shape(sf_engine* e, int k, int c) {
+    int per_sm = 0;
+    int rc = shape_per_sm(e->ctx->device, k, &per_sm);
+    if (rc) return rc;
+    const int blocks = per_sm * e->ctx->num_sms;  // persistent: one wave; CTAs beyond the tile count exit at once
+    if (k != e->shape || c != e->sched || blocks != e->blocks) drop_graph(e);
+    e->shape = k;
+    e->sched = c;
+    e->blocks = blocks;
+    return SF_OK;
+}
+
+// the caller's tile_rows (and tile_schedule) fix the sweeps; tile_rows 0 lets the tuner choose both
+int configure_tuner(sf_engine* e) {
+    int k = DEFAULT_CAND / NSCHED, c = DEFAULT_CAND % NSCHED;
+    const int sc = e->opt.tile_schedule;
+    if (e->opt.tile_rows != 0) {
+        k = shape_of_rows(e->opt.tile_rows);
+        if (k < 0) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_rows must be 0, 8, 16 or 32");
+        if (sc < 0 || sc > NSCHED) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_schedule must be 0, 1 or 2");
+        c = sc == 2 ? 1 : 0;
+        e->tune_state = SF_TUNE_FIXED;
+    } else {
+        if (sc != 0) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_schedule needs tile_rows");
+        e->tune_state = SF_TUNE_MEASURING;
+    }
+    e->tune_trials = 0;
+    e->tune_key = -1;
+    e->timed_pieces = 0;
+    for (double& v : e->tune_ns) v = 0.0;
+    return use_shape(e, k, c);
+}
+
+// workload class of a sweep set: half-octaves of the mean points per instance, octaves of the total points
+int workload_key(const sf_engine* e, const std::vector<int>& ids, double* points) {
+    double tot = 0.0;
+    for (int q : ids) tot += (double)(e->slots[q].d.Nx - 1) * (e->slots[q].d.Ny - 1);
+    *points = tot;
+    const int a = (int)std::floor(2.0 * std::log2(std::max(1.0, tot / (double)ids.size())));
+    const int b = (int)std::floor(std::log2(std::max(1.0, tot)));
+    return a * 128 + b;
+}
+
+// reads the timings of the last round's trial pieces (the stream has been synchronised); once every candidate
+// has had TUNE_PASSES pieces, keeps the fastest and records it for the workload class
+int tuner_collect(sf_engine* e) {
+    if (e->timed_pieces == 0) return SF_OK;
+    for (int i = 0; i < e->timed_pieces; ++i) {
+        float ms = 0.f;
+        SF_CUDA(cudaEventElapsedTime(&ms, e->ev_piece[i], e->ev_piece[i + 1]));
+        const double ns = (double)ms * 1e6 / std::max(1.0, e->timed_points);
+        double& seen = e->tune_ns[(e->timed_first + i) % NCAND];
+        if (seen == 0.0 || ns < seen) seen = ns;
+    }
+    e->tune_trials += e->timed_pieces;
+    e->timed_pieces = 0;
+    if (e->tune_trials < NCAND * TUNE_PASSES) return SF_OK;
+    int best = DEFAULT_CAND;
+    for (int k = 0; k < NCAND; ++k)
+        if (e->tune_ns[k] > 0.0 && e->tune_ns[k] < e->tune_ns[best]) best = k;
+    e->tune_state = SF_TUNE_MEASURED;
+    e->ctx->sweep_shapes[e->tune_key] = best;
+    return use_shape(e, best / NSCHED, best % NSCHED);
+}
+
+// `n` sweeps (launch parities k0, k0 + 1, ...) over the uploaded sweep list of the current shape
+int launch_direct(sf_engine* e, int k0, int n) {
+    const int sk = e->shape;
+    const SweepShape& sh = kShapes[sk];
+    for (int k = k0; k < k0 + n; ++k) {
+        sh.kern<<<e->blocks, dim3(BX, TY), sh.smem, e->s>>>(maps_of(e, sk), e->d_insts, e->d_tiles[sk],
+                                                             e->d_ntiles + sk, k & 1, e->sched, e->d_flag);
+        SF_CHECK_LAUNCH();
+    }
+    return SF_OK;
+}
+
+// a measuring round: its first sweeps run as short timed pieces, one per trial still to run (P sweeps each, P
+// even so that the launch parities run on), the rest in the default candidate; all launched directly, after
+// the lists of every shape are uploaded, so that nothing but sweeps lies between the events
+int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
+    const int K = e->opt.fold_every;
+    const int P = std::min(8, std::max(2, (K / (2 * NCAND)) & ~1));
+    const int pieces = std::min(NCAND * TUNE_PASSES - e->tune_trials, K / P);
+    int rc, k = 0;
+    for (int sk = 0; sk < NSHAPES; ++sk)
+        if ((rc = upload_sweep_list(e, ids, sk))) return rc;
+    SF_CUDA(cudaEventRecord(e->ev_piece[0], e->s));
+    for (int i = 0; i < pieces; ++i, k += P) {
+        const int cand = (e->tune_trials + i) % NCAND;
+        if ((rc = use_shape(e, cand / NSCHED, cand % NSCHED))) return rc;
+        if ((rc = launch_direct(e, k, P))) return rc;
+        SF_CUDA(cudaEventRecord(e->ev_piece[i + 1], e->s));
+    }
+    e->timed_first = e->tune_trials;
+    e->timed_pieces = pieces;
+    e->timed_points = points * P;
+    if (k < K) {
+        if ((rc = use_shape(e, DEFAULT_CAND / NSCHED, DEFAULT_CAND % NSCHED))) return rc;
+        if ((rc = launch_direct(e, k, K - k))) return rc;
+    }
+    return SF_OK;
+}
+
+// one fold's worth of sweeps over the sweep set `ids`, in the shape the tuner (or the caller) chose
+int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
+    const int K = e->opt.fold_every;
+    int rc;
+    if (e->tune_state == SF_TUNE_MEASURING) {
+        double points = 0.0;
+        const int key = workload_key(e, ids, &points);
+        if (e->tune_key < 0) {
+            auto it = e->ctx->sweep_shapes.find(key);
+            if (it != e->ctx->sweep_shapes.end()) {
+                e->tune_state = SF_TUNE_CACHED;
+                if ((rc = use_shape(e, it->second / NSCHED, it->second % NSCHED))) return rc;
+            } else {
+                e->tune_key = key;
+            }
+        }
+        if (e->tune_state == SF_TUNE_MEASURING) {
+            if ((rc = launch_trials(e, ids, points))) return rc;
+            e->ctx->launches += K;
+            e->sweeps += K;
+            return SF_OK;
+        }
+    }
+    if ((rc = upload_sweep_list(e, ids, e->shape))) return rc;
     if (e->opt.use_graphs) {
         if (e->gexec && e->graph_k != K) drop_graph(e);
         if (!e->gexec) {
             SF_CUDA(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
-            int lrc = run();
+            int lrc = launch_direct(e, 0, K);
             cudaGraph_t g = nullptr;
             cudaError_t ce = cudaStreamEndCapture(e->s, &g);
             if (lrc) {
@@ -837,8 +1096,7 @@ int launch_sweeps(sf_engine* e) {
         }
         SF_CUDA(cudaGraphLaunch(e->gexec, e->s));
     } else {
-        int rc = run();
-        if (rc) return rc;
+        if ((rc = launch_direct(e, 0, K))) return rc;
     }
     e->ctx->launches += K;
     e->sweeps += K;
@@ -856,13 +1114,12 @@ int admit(sf_engine* e, int q, sf_batch_instance& u, int dtau_max) {
     I.Nx = (int)u.Nx;
     I.Ny = (int)u.Ny;
     I.ntx = (int)ceil_div(u.Nx - 1, BX);
-    I.nty = (int)ceil_div(u.Ny - 1, BY);
     I.LD32 = I.LD64 = L.LD;
     I.rows = L.rows;
     I.fstride32 = I.fstride64 = L.fstride;
     I.f32 = (float*)(e->arena + h.off);
     I.f64 = (double*)(e->arena + h.off + L.bytes32);
-    h.ntiles = (int64_t)I.ntx * I.nty;
+    h.ntiles64 = (int64_t)I.ntx * ceil_div(u.Ny - 1, BY64);
     const double Vdmp = 4.0, Vsc = 0.45, Ptsc = 0.5;  // StokesSolver_multixpu.jl:17-19
     const int64_t Nx = u.Nx, Ny = u.Ny, LD = L.LD;
     const double mdxy = std::min(u.dx, u.dy);
@@ -904,16 +1161,8 @@ int admit(sf_engine* e, int q, sf_batch_instance& u, int dtau_max) {
         k_rho_scale64<<<1, 1024, 0, s>>>(u.rho_vy, (int)Nx, (int)Ny, u.g_y, e->d_scale + q);
         SF_LAUNCHED(ctx);
     }
-    CUtensorMap maps[M_NUM];
-    const int gmap[M_NUM] = {G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_MUB, G_MUP, G_RHO, G_RDIV,
-                             G_RVX, G_RVY, G_RX, G_RY};
-    for (int m = 0; m < M_NUM; ++m) {
-        const bool halo = m <= M_RDIV;
-        int rc = encode_tmap_f32(&maps[m], I.f32 + (int64_t)gmap[m] * I.fstride32, LD, I.rows, halo ? TW : BX,
-                                 halo ? TH : BY);
-        if (rc) return rc;
-    }
-    SF_CUDA(cudaMemcpyAsync(e->d_maps + (size_t)q * M_NUM, maps, sizeof(maps), cudaMemcpyHostToDevice, s));
+    int rc = encode_maps(e, q);  // sweep tilings in every shape
+    if (rc) return rc;
     SF_CUDA(cudaMemcpyAsync(e->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, s));
     return SF_OK;
 }
@@ -1009,12 +1258,12 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
         SF_LAUNCHED(ctx);
     }
     int64_t nt = 0;
-    if ((rc = upload_lists(e, ids, true, &nt))) return rc;
-    k_maxv64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles, e->d_part);
+    if ((rc = upload_lists64(e, ids, &nt))) return rc;
+    k_maxv64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles64, e->d_part);
     SF_LAUNCHED(ctx);
     k_inst_dt<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_insts, e->d_segs, e->d_part);
     SF_LAUNCHED(ctx);
-    k_resid64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles, e->d_part);
+    k_resid64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles64, e->d_part);
     SF_LAUNCHED(ctx);
     k_inst_err<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_segs, e->d_part, e->d_insts, e->d_scale, e->d_out);
     SF_LAUNCHED(ctx);
@@ -1024,6 +1273,7 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
     int flag = 0;
     memcpy(&flag, e->h_out + ids.size() * 3, sizeof(int));
     if (flag) return fail(SF_ERR_CUDA, "sf_engine: a tile copy did not complete in time");
+    if ((rc = tuner_collect(e))) return rc;
     std::vector<int> sweep;
     bool any_done = false;
     for (size_t k = 0; k < ids.size(); ++k) {
@@ -1058,8 +1308,7 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
         SF_CUDA(cudaStreamWaitEvent(caller, e->ev_out, 0));
     }
     if (sweep.empty()) return SF_OK;
-    if (sweep.size() != ids.size() && (rc = upload_lists(e, sweep, false, &nt))) return rc;
-    if ((rc = launch_sweeps(e))) return rc;
+    if ((rc = launch_sweeps(e, sweep))) return rc;
     for (int q : sweep) {
         e->slots[q].inner_total += e->opt.fold_every;
         e->slots[q].swept = true;
@@ -1157,7 +1406,17 @@ extern "C" int sf_engine_get_stats(sf_engine* e, sf_engine_stats* st) {
     st->sweeps = e->sweeps;
     st->active = active_count(e);
     st->pending_results = (int32_t)e->pending.size();
+    st->tile_rows = kShapes[e->shape].rows;
+    st->tile_schedule = e->sched + 1;
+    st->tune_state = e->tune_state;
+    for (int k = 0; k < NCAND; ++k) st->tune_ns[k] = e->tune_ns[k];
     return SF_OK;
+}
+
+extern "C" int sf_ctx_batch_stats(sf_ctx* ctx, sf_engine_stats* st) {
+    SF_REQUIRE(ctx && st, "sf_ctx_batch_stats: NULL argument");
+    SF_REQUIRE(ctx->batch_engine, "sf_ctx_batch_stats: no batched solve has run in this context");
+    return sf_engine_get_stats(ctx->batch_engine, st);
 }
 
 extern "C" int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst, int n, const sf_mixed_options* o,
@@ -1186,6 +1445,7 @@ extern "C" int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst,
         ctx->batch_engine = e;
     }
     e->opt = normalized(o);
+    if ((rc = configure_tuner(e))) return rc;
     if ((rc = ensure(ctx, ctx->mixed, (size_t)total))) return rc;
     e->arena = (unsigned char*)ctx->mixed.ptr;
     e->alloc.reset(total);

@@ -59,6 +59,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint64
     }
 }
 
+// A tensor map that the host copied into global memory (between launches) is seen by this thread's
+// bulk-tensor copies only after this fence; once per thread block and map, until the map changes again.
+// System scope, because the host wrote the map (device scope measured no cheaper).
+__device__ __forceinline__ void fence_tensormap_acquire(const CUtensorMap* map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"((uint64_t)map) : "memory");
+}
+
 // 2-D tiled bulk-tensor load global -> shared, completion counted on `bar`.
 // No multicast: the tile lands in this CTA's shared memory only.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {

@@ -8,7 +8,7 @@ Julia functions on CUDA tensors (``api``) and the timestep driver
 (``driver``).  There is no CPU fallback.
 """
 from ._lib import LIB_PATH, StokesFlowError, build, lib  # noqa: F401
-from .api import (Context, Engine, MixedProblem, PlumeModel, bilinear_marker_to_grid,  # noqa: F401
+from .api import (Context, Engine, MixedProblem, PlumeModel, batch_stats, bilinear_marker_to_grid,  # noqa: F401
                   bilinear_marker_to_grid_noalloc, default_context, get_warnings, initialize_markers,
                   initialize_markers_host, marker_count, mixed_options, move_markers_rk4, rebin_markers,
                   residual_scale, set_initial_marker_properties, solve_stokes, solve_stokes_batch_mixed,

@@ -23,6 +23,11 @@ SF_ERR_NONFINITE = 5
 SF_ERR_TOO_LARGE = 6
 SF_ERR_BUSY = 7
 
+# sf_engine_stats.tune_state
+TUNE_STATES = {0: "fixed", 1: "measuring", 2: "measured", 3: "cached"}
+# sf_mixed_options.tile_schedule / sf_engine_stats.tile_schedule
+SCHEDULES = {1: "strided", 2: "chunked"}
+
 # limits of the allocation-free deposit (include/stokesflow_b200.h)
 SF_NOALLOC_MAX_MARKERS = 1048576
 SF_NOALLOC_MAX_CELLS = 262144
@@ -71,16 +76,25 @@ class BatchInstance(C.Structure):
 class MixedOptions(C.Structure):
     """sf_mixed_options."""
     _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32), ("dtau_local_max", _i32),
-                ("retry_local_max", _i32)]
+                ("retry_local_max", _i32), ("tile_rows", _i32), ("tile_schedule", _i32)]
 
 
 class EngineStats(C.Structure):
     """sf_engine_stats."""
     _fields_ = [("arena_bytes", _i64), ("arena_used", _i64), ("arena_peak", _i64), ("submitted", _i64),
-                ("finished", _i64), ("rounds", _i64), ("sweeps", _i64), ("active", _i32), ("pending_results", _i32)]
+                ("finished", _i64), ("rounds", _i64), ("sweeps", _i64), ("active", _i32), ("pending_results", _i32),
+                ("tile_rows", _i32), ("tile_schedule", _i32), ("tune_state", _i32), ("reserved", _i32),
+                ("tune_ns", _d * 6)]
+
+    CANDIDATES = ((8, "strided"), (8, "chunked"), (16, "strided"), (16, "chunked"), (32, "strided"),
+                  (32, "chunked"))
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d["tune_ns"] = dict(zip(self.CANDIDATES, list(self.tune_ns)))
+        d["tile_schedule"] = SCHEDULES.get(self.tile_schedule, self.tile_schedule)
+        d["tune_state"] = TUNE_STATES.get(self.tune_state, self.tune_state)
+        return d
 
 
 class Domain(C.Structure):
@@ -137,6 +151,7 @@ PROTOTYPES = {
     "sf_engine_submit": (C.c_int, [_vp, C.POINTER(BatchInstance), _vp, C.POINTER(_i64)]),
     "sf_engine_step": (C.c_int, [_vp, _vp, C.POINTER(_i64), _i32, C.POINTER(_i32), C.POINTER(_i32)]),
     "sf_engine_get_stats": (C.c_int, [_vp, C.POINTER(EngineStats)]),
+    "sf_ctx_batch_stats": (C.c_int, [_vp, C.POINTER(EngineStats)]),
     "sf_move_markers_rk4": (C.c_int, [_vp, _pd, _pd, _i64, _pd, _i64, _i64, _pd, _i64, _i64, _d, _d, _d, _d, _d, _d,
                                       _d, _d, _d, _vp]),
     "sf_rebin_markers": (C.c_int, [_vp, _pd, _pd, _i64, _d, _d, _d, _d, _i64, _i64, _pd, _pd, _pd, _vp]),

@@ -36,7 +36,7 @@ from ._lib import check, lib
 __all__ = ["Context", "default_context", "zeros", "bilinear_marker_to_grid", "solve_stokes", "solve_stokes_info",
            "residual_scale", "move_markers_rk4", "rebin_markers", "marker_count", "initialize_markers",
            "initialize_markers_host", "set_initial_marker_properties", "get_warnings", "PlumeModel", "MixedProblem",
-           "mixed_options", "solve_stokes_batch_mixed", "Engine", "bilinear_marker_to_grid_noalloc"]
+           "mixed_options", "batch_stats", "solve_stokes_batch_mixed", "Engine", "bilinear_marker_to_grid_noalloc"]
 
 
 class Context:
@@ -231,13 +231,25 @@ class MixedProblem:
 
 
 def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True, dtau_local_max=False,
-                  retry_local_max=True):
+                  retry_local_max=True, tile_rows=0, tile_schedule=None):
     """Options of the mixed-precision / batched solver (sf_mixed_options).  dtau_local_max: pseudo-time
     steps from the stencil's largest viscosity instead of the reference's average (faster on soft
     inclusions); the converged solution is the same.  retry_local_max: an instance that diverges restarts
-    from its inputs with the stencil-maximum step."""
+    from its inputs with the stencil-maximum step.  tile_rows: 8, 16 or 32 rows per sweep tile, or 0 for
+    the autotuner's choice of rows and schedule (every choice gives the same bits); tile_schedule
+    ("strided" or "chunked") goes with a fixed tile_rows."""
+    sched = {None: 0, "strided": 1, "chunked": 2}[tile_schedule]
     return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)), int(bool(dtau_local_max)),
-                             int(bool(retry_local_max)))
+                             int(bool(retry_local_max)), int(tile_rows), sched)
+
+
+def batch_stats(ctx: Context | None = None) -> dict:
+    """Stats of the engine behind the context's last batched / mixed solve (sf_ctx_batch_stats): the sweep
+    tile rows and schedule in use, the tuner's state and its measured ns per point-sweep of each candidate
+    ((rows, schedule) -> ns)."""
+    s = _lib.EngineStats()
+    check(lib().sf_ctx_batch_stats(_ctx(ctx).handle, C.byref(s)), "sf_ctx_batch_stats")
+    return s.as_dict()
 
 
 def solve_stokes_batch_mixed(problems, *, options=None, ctx: Context | None = None, stream=None):
