@@ -70,11 +70,11 @@ def parse():
     ap.add_argument("--pt32-probe", type=int, default=0, metavar="SWEEPS",
                     help="kernel probe: one n x n instance through the mixed engine for exactly SWEEPS FP32 sweeps "
                          "(one fold); prints the sweep time; used for ncu captures of k_pt32")
-    ap.add_argument("--form", default="timestep", choices=["timestep", "precision", "batch", "serve"],
+    ap.add_argument("--form", default="timestep", choices=["timestep", "precision", "batch", "serve", "tune"],
                     help="timestep: the plain FP64 timestep (default line); precision: the same timesteps with FP32 "
                          "sweeps + FP64 correction beside the plain path; batch: many independent solves in one "
                          "engine vs a loop of plain FP64 solves; serve: a Poisson request stream, continuous "
-                         "batching vs plain FP64 serving")
+                         "batching vs plain FP64 serving; tune: the sweep tuner's table of tile shapes and schedules")
     ap.add_argument("--precision-cases", type=int, default=2, help="precision form: plume contrasts drawn from seed")
     ap.add_argument("--precision-contrast", default="0,2",
                     help="precision form: log10 range of matrix/plume viscosity, log-uniform (soft plume)")
@@ -138,7 +138,9 @@ def pt32_probe(a):
     for arr in (rho, mub, mup):
         arr.copy_(1.0 + 0.5 * torch.rand(arr.shape[1], arr.shape[0], device="cuda", dtype=torch.float64,
                                          generator=g).t())
-    opts = sf.mixed_options(max_sweeps=sweeps, fold_every=sweeps)
+    # a fixed sweep shape (16 rows strided unless given), so that every launch is the same kernel
+    opts = sf.mixed_options(max_sweeps=sweeps, fold_every=sweeps, tile_rows=a.tile_rows or 16,
+                            tile_schedule=a.tile_schedule if a.tile_rows else "strided")
     h = 1.0 / (n - 1)
     for rep in range(2):   # the first run captures the graph
         p = sf.MixedProblem(P, Vx, Vy, rho, mub, mup, Vxs, Vys, 9.81, h, h, n, n, 0.0, 0.5, eps=1e-300)
@@ -150,6 +152,47 @@ def pt32_probe(a):
     print(json.dumps({"probe": "k_pt32", "n": n, "sweeps": r["inner_iters"], "us_per_sweep": round(us, 3),
                       "gpts_per_s": round(pts / us / 1e3, 2), "t_eff_gbs": round(gbs, 1),
                       "frac_of_peak": round(gbs / peak, 4), "peak_source": src}), flush=True)
+
+
+def run_tune_form(a):
+    """The sweep autotuner's candidate table: G point-sweeps/s of each tile shape (8, 16, 32 rows) and schedule
+    (strided, chunked) as the engine times them in its first round, on (1) the instance sizes of the batch
+    form's workload and (2) one n x n instance.  Smooth random fields; 2 folds of fold_every sweeps each."""
+    import stokesflow_b200 as sf
+    from stokesflow_b200 import workloads
+    torch.cuda.set_device(0)
+    g = torch.Generator(device="cuda").manual_seed(a.seed)
+
+    def problem(nx, ny):
+        z = sf.zeros
+        arr = dict(P=z(nx - 1, ny - 1), Vx=z(nx + 2, ny + 1), Vy=z(nx + 1, ny + 2), Vxs=z(nx, ny + 1),
+                   Vys=z(nx + 1, ny), rho=z(nx + 1, ny), mub=z(nx, ny), mup=z(nx - 1, ny - 1))
+        for k in ("rho", "mub", "mup"):
+            t = arr[k]
+            t.copy_(1.0 + 0.5 * torch.rand(t.shape[1], t.shape[0], device="cuda", dtype=torch.float64,
+                                           generator=g).t())
+        p = sf.MixedProblem(arr["P"], arr["Vx"], arr["Vy"], arr["rho"], arr["mub"], arr["mup"], arr["Vxs"],
+                            arr["Vys"], 9.81, 1.0 / (nx - 1), 1.0 / (ny - 1), nx, ny, 0.0, 0.5, eps=1e-300)
+        return p, arr
+
+    specs = workloads.batch_specs(a.batch_instances, a.seed, cells=_pair(a.batch_cells, int))
+    cases = {f"batch {len(specs)} instances, cells {a.batch_cells}": [(sp.Nx, sp.Ny) for sp in specs],
+             f"one instance {a.n}x{a.n}": [(a.n, a.n)]}
+    opts = sf.mixed_options(max_sweeps=2 * a.fold_every, fold_every=a.fold_every)
+    out = {}
+    for name, sizes in cases.items():
+        ctx = sf.Context(0)                  # a fresh context: no choice recorded yet
+        made = [problem(nx, ny) for nx, ny in sizes]
+        sf.solve_stokes_batch_mixed([p for p, _ in made], options=opts, ctx=ctx)
+        st = sf.batch_stats(ctx)
+        out[name] = {"chosen": f"{st['tile_rows']} rows {st['tile_schedule']}", "tuner": st["tune_state"],
+                     "grid_points": int(sum((nx - 1) * (ny - 1) for nx, ny in sizes)),
+                     "gpts_per_s": {k: round(1.0 / v, 2) for k, v in st["tune_ns"].items() if v > 0}}
+        del made
+        torch.cuda.empty_cache()
+    return {"form": "tune", "metric": "FP32 sweep throughput per tile shape and schedule, as the engine's tuner "
+                                      "times it", "unit": "G point-sweeps/s", "cases": out,
+            "data": "synthetic (smooth random fields, seeded)", "fold_every": a.fold_every, "seed": a.seed}
 
 
 def bench_config(a):
@@ -565,8 +608,7 @@ def run_batch_form(a):
             "vs_tight_fp64": tight,
             "nonfinite_instances": [q for q, r in enumerate(res) if r["status"] == 5],
             "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"], "tuner": tiles["tune_state"],
-                            "gpts_per_s_timed": {f"{r}/{c}": round(1.0 / v, 2) for (r, c), v in tiles["tune_ns"].items()
-                                                 if v > 0}},
+                            "gpts_per_s_timed": {k: round(1.0 / v, 2) for k, v in tiles["tune_ns"].items() if v > 0}},
             "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
             "clocks": clk,
             "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {a.batch_cells}, 9-25 "
@@ -663,7 +705,8 @@ def main():
         return
     if a.form != "timestep" and a.impl == "ours":
         if rank == 0:
-            run = {"precision": run_precision_form, "batch": run_batch_form, "serve": run_serve_form}[a.form]
+            run = {"precision": run_precision_form, "batch": run_batch_form, "serve": run_serve_form,
+                   "tune": run_tune_form}[a.form]
             print(json.dumps(run(a)), flush=True)
         return
     if a.impl == "reference":

@@ -86,8 +86,7 @@ class EngineStats(C.Structure):
                 ("tile_rows", _i32), ("tile_schedule", _i32), ("tune_state", _i32), ("reserved", _i32),
                 ("tune_ns", _d * 6)]
 
-    CANDIDATES = ((8, "strided"), (8, "chunked"), (16, "strided"), (16, "chunked"), (32, "strided"),
-                  (32, "chunked"))
+    CANDIDATES = ("8/strided", "8/chunked", "16/strided", "16/chunked", "32/strided", "32/chunked")
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

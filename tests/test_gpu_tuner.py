@@ -59,7 +59,7 @@ def test_every_shape_and_the_tuner_give_the_same_bits(sf):
     got, res, st = solve(sf, ctx, 0)               # the tuner times every candidate while it solves
     assert st["tune_state"] == "measured", st
     assert all(v > 0 for v in st["tune_ns"].values())
-    assert (st["tile_rows"], st["tile_schedule"]) == min(st["tune_ns"], key=st["tune_ns"].get)
+    assert f'{st["tile_rows"]}/{st["tile_schedule"]}' == min(st["tune_ns"], key=st["tune_ns"].get)
     assert same(got, ref), "the tuned solve differs"
     chosen = (st["tile_rows"], st["tile_schedule"])
     got, res, st = solve(sf, ctx, 0)               # same workload class: the context remembers
