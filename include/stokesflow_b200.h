@@ -307,12 +307,14 @@ typedef struct {
                                   max_sweeps); it converges on mixed soft/stiff layouts where the
                                   reference's step diverges.  Instances that converge are unaffected (1) */
     int32_t tile_rows;         /* rows of the 32-column sweep tiles: 8, 16 or 32, or 0 to let the
-                                  autotuner choose the rows and the schedule.  The tuner times the first
-                                  rounds' sweeps in every shape and schedule (two rounds each), keeps the
-                                  fastest per point, and records it in the context for the workload class
-                                  (mean and total grid points), so later solves of that class start with
-                                  it.  Every shape and schedule computes the same bits, so the choice
-                                  changes the speed only (0)                                          */
+                                  autotuner choose the rows and the schedule.  Each round's sweep set has
+                                  a workload class (half-octave of the mean, octave of the total grid
+                                  points).  The first round of a class the context has not seen begins
+                                  with short timed pieces of every shape and schedule (two each); the
+                                  fastest per point is then used and recorded in the context, so later
+                                  rounds and solves of that class take it at once.  Every shape and
+                                  schedule computes the same bits, so the choice changes the speed
+                                  only (0)                                                            */
     int32_t tile_schedule;     /* with tile_rows set: 1 strided (CTA b of G takes tiles b, b+G, ...),
                                   2 chunked (CTA b takes one contiguous run of tiles); 0 = 1.  With
                                   tile_rows 0 it must be 0 (0)                                        */
@@ -374,10 +376,12 @@ typedef struct {
     int32_t pending_results;   /* finished, not yet reported by sf_engine_step   */
     int32_t tile_rows;         /* rows of the sweep tiles in use                 */
     int32_t tile_schedule;     /* 1 strided, 2 chunked                           */
-    int32_t tune_state;        /* SF_TUNE_*                                      */
-    int32_t reserved;
-    double tune_ns[6];         /* best measured ns per point-sweep of 8 rows strided, 8 chunked, 16
-                                  strided, 16 chunked, 32 strided, 32 chunked (0: not timed) */
+    int32_t tune_state;        /* SF_TUNE_* for the current workload class       */
+    int32_t tune_classes;      /* workload classes with a recorded choice in the context */
+    int64_t tune_rounds;       /* rounds whose sweeps began with timed trial pieces */
+    int64_t tune_hits;         /* workload-class changes answered from the context's record */
+    double tune_ns[6];         /* the last completed measurement: ns per point-sweep of 8 rows strided,
+                                  8 chunked, 16 strided, 16 chunked, 32 strided, 32 chunked (0: none) */
 } sf_engine_stats;
 
 /* Arena bytes one instance of Nx x Ny grid points holds while admitted. */

@@ -75,7 +75,9 @@ enum { G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_RVX, G_RVY, G_MUB, G_MUP, G_RHO
 // FP64 fields of an instance (each LD64 x rows doubles)
 enum { D_VX, D_VY, D_P, D_RHO, D_MUB, D_MUP, D_NUM };
 // tensor maps per instance, in the order a stage is filled
-enum { M_VXA, M_VXB, M_VYA, M_VYB, M_PA, M_PB, M_MUB, M_MUP, M_RHO, M_RDIV, M_RVX, M_RVY, M_RX, M_RY, M_NUM };
+// tensor maps per instance and shape: all G_NUM FP32 fields as one 3-D tensor (the field index is z), read
+// through a halo box and through a tile box
+enum { M_HALO, M_TILE, M_NUM };
 
 struct Inst {  // device-side description of one instance
     int Nx, Ny;
@@ -131,28 +133,27 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         const Inst& I = insts[td.x];
         const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
         const int in = (I.parity ^ launch_parity) & 1;
-        const CUtensorMap* M = maps + (int64_t)td.x * M_NUM;
+        const CUtensorMap* H = maps + (int64_t)td.x * M_NUM + M_HALO;
+        const CUtensorMap* T = maps + (int64_t)td.x * M_NUM + M_TILE;
         if (td.x != fenced) {
-            fence_tensormap_acquire(&M[in ? M_VXB : M_VXA]);
-            fence_tensormap_acquire(&M[in ? M_VYB : M_VYA]);
-            fence_tensormap_acquire(&M[in ? M_PB : M_PA]);
-            for (int m = M_MUB; m < M_NUM; ++m) fence_tensormap_acquire(&M[m]);
+            fence_tensormap_acquire(H);
+            fence_tensormap_acquire(T);
             fenced = td.x;
         }
         unsigned char* st = smem + s * STAGE_BYTES;
         mbar_arrive_expect_tx(&bar[s], STAGE_TX);
-        tma_load_2d(st + 0 * HALO_BYTES, &M[in ? M_VXB : M_VXA], &bar[s], i0, j0);
-        tma_load_2d(st + 1 * HALO_BYTES, &M[in ? M_VYB : M_VYA], &bar[s], i0, j0);
-        tma_load_2d(st + 2 * HALO_BYTES, &M[in ? M_PB : M_PA], &bar[s], i0, j0);
-        tma_load_2d(st + 3 * HALO_BYTES, &M[M_MUB], &bar[s], i0, j0);
-        tma_load_2d(st + 4 * HALO_BYTES, &M[M_MUP], &bar[s], i0, j0);
-        tma_load_2d(st + 5 * HALO_BYTES, &M[M_RHO], &bar[s], i0, j0);
-        tma_load_2d(st + 6 * HALO_BYTES, &M[M_RDIV], &bar[s], i0, j0);
+        tma_load_3d(st + 0 * HALO_BYTES, H, &bar[s], i0, j0, in ? G_VXB : G_VXA);
+        tma_load_3d(st + 1 * HALO_BYTES, H, &bar[s], i0, j0, in ? G_VYB : G_VYA);
+        tma_load_3d(st + 2 * HALO_BYTES, H, &bar[s], i0, j0, in ? G_PB : G_PA);
+        tma_load_3d(st + 3 * HALO_BYTES, H, &bar[s], i0, j0, G_MUB);
+        tma_load_3d(st + 4 * HALO_BYTES, H, &bar[s], i0, j0, G_MUP);
+        tma_load_3d(st + 5 * HALO_BYTES, H, &bar[s], i0, j0, G_RHO);
+        tma_load_3d(st + 6 * HALO_BYTES, H, &bar[s], i0, j0, G_RDIV);
         unsigned char* tb = st + NHALO * HALO_BYTES;
-        tma_load_2d(tb + 0 * TILE_BYTES, &M[M_RVX], &bar[s], i0, j0);
-        tma_load_2d(tb + 1 * TILE_BYTES, &M[M_RVY], &bar[s], i0, j0);
-        tma_load_2d(tb + 2 * TILE_BYTES, &M[M_RX], &bar[s], i0, j0);
-        tma_load_2d(tb + 3 * TILE_BYTES, &M[M_RY], &bar[s], i0, j0);
+        tma_load_3d(tb + 0 * TILE_BYTES, T, &bar[s], i0, j0, G_RVX);
+        tma_load_3d(tb + 1 * TILE_BYTES, T, &bar[s], i0, j0, G_RVY);
+        tma_load_3d(tb + 2 * TILE_BYTES, T, &bar[s], i0, j0, G_RX);
+        tma_load_3d(tb + 3 * TILE_BYTES, T, &bar[s], i0, j0, G_RY);
     };
     // schedule: strided (CTA b takes tiles b, b + G, ...: neighbouring tiles run side by side) or chunked (CTA b
     // takes a contiguous run of ceil(ntiles / G) tiles: it meets few instances, so it fences few maps)
@@ -778,9 +779,10 @@ struct sf_engine {
     std::vector<Seg> h_segs;
     int h_ntiles[NSHAPES] = {};          // sources of the tile-count uploads
     std::vector<int2> h_list[NSHAPES];   // sources of the sweep-list uploads
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    int graph_k = 0;
+    // one captured run of fold_every sweeps per candidate (shape x schedule), kept while its pointers hold
+    cudaGraph_t graph[NCAND] = {};
+    cudaGraphExec_t gexec[NCAND] = {};
+    int graph_k[NCAND] = {};
     int blocks = 0;                      // persistent CTAs of the current shape
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     // sweep shape and its autotuner: while measuring, each round's sweeps run in the next shape to try and are
@@ -796,6 +798,8 @@ struct sf_engine {
     double timed_points = 0.0;           // each piece over this many point-sweeps
     cudaEvent_t ev_piece[NCAND * TUNE_PASSES + 1] = {};
     int64_t next_ticket = 0, submitted = 0, finished = 0, rounds = 0, sweeps = 0;
+    int64_t tune_rounds = 0, tune_hits = 0;   // measuring rounds; class changes answered from the context
+    double trial_ns[NCAND] = {};         // the measurement in progress (tune_ns: the last completed one)
     std::deque<int64_t> pending;
 };
 
@@ -803,11 +807,15 @@ namespace {
 
 CUtensorMap* maps_of(sf_engine* e, int k) { return e->d_maps + (size_t)k * e->slots.size() * M_NUM; }
 
+void drop_graph(sf_engine* e, int c) {
+    if (e->gexec[c]) cudaGraphExecDestroy(e->gexec[c]);
+    if (e->graph[c]) cudaGraphDestroy(e->graph[c]);
+    e->gexec[c] = nullptr;
+    e->graph[c] = nullptr;
+}
+
 void drop_graph(sf_engine* e) {
-    if (e->gexec) cudaGraphExecDestroy(e->gexec);
-    if (e->graph) cudaGraphDestroy(e->graph);
-    e->gexec = nullptr;
-    e->graph = nullptr;
+    for (int c = 0; c < NCAND; ++c) drop_graph(e, c);
 }
 
 void engine_free(sf_engine* e) {
@@ -912,7 +920,8 @@ int upload_lists64(sf_engine* e, const std::vector<int>& ids, int64_t* nt_out) {
 int upload_sweep_list(sf_engine* e, const std::vector<int>& ids, int k) {
     int64_t nt = 0;
     for (int q : ids) nt += e->slots[q].ntiles[k];
-    if (nt > e->tile_cap[k]) drop_graph(e);  // the graph may hold the old pointer
+    if (nt > e->tile_cap[k])  // the shape's graphs hold the old pointer
+        for (int c = 0; c < NSCHED; ++c) drop_graph(e, k * NSCHED + c);
     int rc = grow_list(e, nt, &e->d_tiles[k], nullptr, &e->tile_cap[k]);
     if (rc) return rc;
     std::vector<int2>& h = e->h_list[k];
@@ -926,23 +935,18 @@ int upload_sweep_list(sf_engine* e, const std::vector<int>& ids, int k) {
     return SF_OK;
 }
 
-// sweep tilings of slot q: its tile count and its 14 tensor maps (box = tile + halo, or tile) in every shape,
+// sweep tilings of slot q: its tile count and its 2 tensor maps (box = tile + halo, or tile) in every shape,
 // encoded once at admission, so that a change of shape is a choice of pointers
 int encode_maps(sf_engine* e, int q) {
     Slot& h = e->slots[q];
     const Inst& I = h.d;
-    const int gmap[M_NUM] = {G_VXA, G_VXB, G_VYA, G_VYB, G_PA, G_PB, G_MUB, G_MUP, G_RHO, G_RDIV,
-                             G_RVX, G_RVY, G_RX, G_RY};
     CUtensorMap maps[M_NUM];
     for (int k = 0; k < NSHAPES; ++k) {
         const int rows = kShapes[k].rows;
         h.ntiles[k] = (int64_t)I.ntx * ceil_div(I.Ny - 1, rows);
-        for (int m = 0; m < M_NUM; ++m) {
-            const bool halo = m <= M_RDIV;
-            int rc = encode_tmap_f32(&maps[m], I.f32 + (int64_t)gmap[m] * I.fstride32, I.LD32, I.rows,
-                                     halo ? TW : BX, halo ? rows + 2 : rows);
-            if (rc) return rc;
-        }
+        int rc = encode_tmap_f32_fields(&maps[M_HALO], I.f32, I.LD32, I.rows, G_NUM, I.fstride32, TW, rows + 2);
+        if (rc || (rc = encode_tmap_f32_fields(&maps[M_TILE], I.f32, I.LD32, I.rows, G_NUM, I.fstride32, BX, rows)))
+            return rc;
         // pageable source: staged before the call returns, so `maps` is free again
         SF_CUDA(cudaMemcpyAsync(maps_of(e, k) + (size_t)q * M_NUM, maps, sizeof(maps), cudaMemcpyHostToDevice, e->s));
     }
@@ -955,8 +959,7 @@ int use_shape(sf_engine* e, int k, int c) {
     int rc = shape_per_sm(e->ctx->device, k, &per_sm);
     if (rc) return rc;
     const int blocks = per_sm * e->ctx->num_sms;  // persistent: one wave; CTAs beyond the tile count exit at once
-    if (k != e->shape || c != e->sched || blocks != e->blocks) drop_graph(e);
-    e->shape = k;
+    e->shape = k;  // each candidate's graph was captured with its own grid, maps and list
     e->sched = c;
     e->blocks = blocks;
     return SF_OK;
@@ -979,7 +982,9 @@ int configure_tuner(sf_engine* e) {
     e->tune_trials = 0;
     e->tune_key = -1;
     e->timed_pieces = 0;
+    e->tune_rounds = e->tune_hits = 0;
     for (double& v : e->tune_ns) v = 0.0;
+    for (double& v : e->trial_ns) v = 0.0;
     return use_shape(e, k, c);
 }
 
@@ -1001,7 +1006,7 @@ int tuner_collect(sf_engine* e) {
         float ms = 0.f;
         SF_CUDA(cudaEventElapsedTime(&ms, e->ev_piece[i], e->ev_piece[i + 1]));
         const double ns = (double)ms * 1e6 / std::max(1.0, e->timed_points);
-        double& seen = e->tune_ns[(e->timed_first + i) % NCAND];
+        double& seen = e->trial_ns[(e->timed_first + i) % NCAND];
         if (seen == 0.0 || ns < seen) seen = ns;
     }
     e->tune_trials += e->timed_pieces;
@@ -1009,7 +1014,8 @@ int tuner_collect(sf_engine* e) {
     if (e->tune_trials < NCAND * TUNE_PASSES) return SF_OK;
     int best = DEFAULT_CAND;
     for (int k = 0; k < NCAND; ++k)
-        if (e->tune_ns[k] > 0.0 && e->tune_ns[k] < e->tune_ns[best]) best = k;
+        if (e->trial_ns[k] > 0.0 && e->trial_ns[k] < e->trial_ns[best]) best = k;
+    for (int k = 0; k < NCAND; ++k) e->tune_ns[k] = e->trial_ns[k];
     e->tune_state = SF_TUNE_MEASURED;
     e->ctx->sweep_shapes[e->tune_key] = best;
     return use_shape(e, best / NSCHED, best % NSCHED);
@@ -1034,7 +1040,9 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     const int K = e->opt.fold_every;
     const int P = std::min(8, std::max(2, (K / (2 * NCAND)) & ~1));
     const int pieces = std::min(NCAND * TUNE_PASSES - e->tune_trials, K / P);
+    const int prev_shape = e->shape, prev_sched = e->sched;
     int rc, k = 0;
+    ++e->tune_rounds;
     for (int sk = 0; sk < NSHAPES; ++sk)
         if ((rc = upload_sweep_list(e, ids, sk))) return rc;
     SF_CUDA(cudaEventRecord(e->ev_piece[0], e->s));
@@ -1047,8 +1055,8 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     e->timed_first = e->tune_trials;
     e->timed_pieces = pieces;
     e->timed_points = points * P;
-    if (k < K) {
-        if ((rc = use_shape(e, DEFAULT_CAND / NSCHED, DEFAULT_CAND % NSCHED))) return rc;
+    if (k < K) {  // the rest in the choice made before (the previous class's, or the default)
+        if ((rc = use_shape(e, prev_shape, prev_sched))) return rc;
         if ((rc = launch_direct(e, k, K - k))) return rc;
     }
     return SF_OK;
@@ -1058,16 +1066,22 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
 int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
     const int K = e->opt.fold_every;
     int rc;
-    if (e->tune_state == SF_TUNE_MEASURING) {
+    if (e->tune_state != SF_TUNE_FIXED) {
+        // the workload class of this round's sweep set; a new class takes the context's recorded choice, or
+        // is measured now (a batch that drains and a serving mix move through classes)
         double points = 0.0;
         const int key = workload_key(e, ids, &points);
-        if (e->tune_key < 0) {
+        if (key != e->tune_key) {
+            e->tune_key = key;
+            e->tune_trials = 0;
+            for (double& v : e->trial_ns) v = 0.0;
             auto it = e->ctx->sweep_shapes.find(key);
             if (it != e->ctx->sweep_shapes.end()) {
                 e->tune_state = SF_TUNE_CACHED;
+                ++e->tune_hits;
                 if ((rc = use_shape(e, it->second / NSCHED, it->second % NSCHED))) return rc;
             } else {
-                e->tune_key = key;
+                e->tune_state = SF_TUNE_MEASURING;
             }
         }
         if (e->tune_state == SF_TUNE_MEASURING) {
@@ -1079,8 +1093,9 @@ int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
     }
     if ((rc = upload_sweep_list(e, ids, e->shape))) return rc;
     if (e->opt.use_graphs) {
-        if (e->gexec && e->graph_k != K) drop_graph(e);
-        if (!e->gexec) {
+        const int c = e->shape * NSCHED + e->sched;
+        if (e->gexec[c] && e->graph_k[c] != K) drop_graph(e, c);
+        if (!e->gexec[c]) {
             SF_CUDA(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
             int lrc = launch_direct(e, 0, K);
             cudaGraph_t g = nullptr;
@@ -1090,11 +1105,11 @@ int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
                 return lrc;
             }
             SF_CUDA(ce);
-            e->graph = g;
-            SF_CUDA(cudaGraphInstantiate(&e->gexec, g, 0));
-            e->graph_k = K;
+            e->graph[c] = g;
+            SF_CUDA(cudaGraphInstantiate(&e->gexec[c], g, 0));
+            e->graph_k[c] = K;
         }
-        SF_CUDA(cudaGraphLaunch(e->gexec, e->s));
+        SF_CUDA(cudaGraphLaunch(e->gexec[c], e->s));
     } else {
         if ((rc = launch_direct(e, 0, K))) return rc;
     }
@@ -1409,6 +1424,9 @@ extern "C" int sf_engine_get_stats(sf_engine* e, sf_engine_stats* st) {
     st->tile_rows = kShapes[e->shape].rows;
     st->tile_schedule = e->sched + 1;
     st->tune_state = e->tune_state;
+    st->tune_classes = (int32_t)e->ctx->sweep_shapes.size();
+    st->tune_rounds = e->tune_rounds;
+    st->tune_hits = e->tune_hits;
     for (int k = 0; k < NCAND; ++k) st->tune_ns[k] = e->tune_ns[k];
     return SF_OK;
 }

@@ -583,8 +583,7 @@ int encode_tmap_f32(CUtensorMap* map, const float* base, int64_t ld, int64_t row
     return encode_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ld, rows, box_w, box_h);
 }
 
-static int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int esize, const void* base, int64_t ld,
-                       int64_t rows, int box_w, int box_h) {
+static int get_encoder(PFN_encodeTiled* out) {
     static PFN_encodeTiled fn = nullptr;
     if (!fn) {
         void* p = nullptr;
@@ -594,15 +593,36 @@ static int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int esize, c
             return fail(SF_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
         fn = (PFN_encodeTiled)p;
     }
-    cuuint64_t dims[2] = {(cuuint64_t)ld, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)ld * (cuuint64_t)esize};
-    cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = fn(map, dtype, 2, (void*)base, dims, strides, box, estr,
+    *out = fn;
+    return SF_OK;
+}
+
+// rank 2 (a field of rows x ld elements) or rank 3 (nfields such fields, fstride elements apart); box depth 1
+static int encode_tiled(CUtensorMap* map, CUtensorMapDataType dtype, int esize, const void* base, int64_t ld,
+                        int64_t rows, int64_t nfields, int64_t fstride, int box_w, int box_h) {
+    PFN_encodeTiled fn = nullptr;
+    int rc = get_encoder(&fn);
+    if (rc) return rc;
+    const cuuint32_t rank = nfields > 0 ? 3 : 2;
+    cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)rows, (cuuint64_t)(nfields > 0 ? nfields : 1)};
+    cuuint64_t strides[2] = {(cuuint64_t)ld * (cuuint64_t)esize, (cuuint64_t)fstride * (cuuint64_t)esize};
+    cuuint32_t box[3] = {(cuuint32_t)box_w, (cuuint32_t)box_h, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dtype, rank, (void*)base, dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(SF_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) + ")");
     return SF_OK;
+}
+
+static int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int esize, const void* base, int64_t ld,
+                       int64_t rows, int box_w, int box_h) {
+    return encode_tiled(map, dtype, esize, base, ld, rows, 0, 0, box_w, box_h);
+}
+
+int encode_tmap_f32_fields(CUtensorMap* map, const float* base, int64_t ld, int64_t rows, int64_t nfields,
+                           int64_t fstride, int box_w, int box_h) {
+    return encode_tiled(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, ld, rows, nfields, fstride, box_w, box_h);
 }
 
 struct Solver {

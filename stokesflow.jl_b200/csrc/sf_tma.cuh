@@ -75,9 +75,21 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+// 3-D tiled bulk-tensor load (x, y, z) global -> shared, completion counted on `bar`; no multicast
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
 // host: encode a 2-D FP64 tensor map over a (rows x ld) row-major buffer
 // (inner dimension ld elements, row pitch ld*8 bytes), box = box_w x box_h.
 int encode_tmap_f64(CUtensorMap* map, const double* base, int64_t ld, int64_t rows, int box_w, int box_h);
 int encode_tmap_f32(CUtensorMap* map, const float* base, int64_t ld, int64_t rows, int box_w, int box_h);
+// host: a 3-D FP32 tensor map over nfields such buffers, fstride elements apart (the field is the z
+// coordinate), box = box_w x box_h x 1
+int encode_tmap_f32_fields(CUtensorMap* map, const float* base, int64_t ld, int64_t rows, int64_t nfields,
+                           int64_t fstride, int box_w, int box_h);
 
 }  // namespace sf

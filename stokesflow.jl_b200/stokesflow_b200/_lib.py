@@ -83,13 +83,13 @@ class EngineStats(C.Structure):
     """sf_engine_stats."""
     _fields_ = [("arena_bytes", _i64), ("arena_used", _i64), ("arena_peak", _i64), ("submitted", _i64),
                 ("finished", _i64), ("rounds", _i64), ("sweeps", _i64), ("active", _i32), ("pending_results", _i32),
-                ("tile_rows", _i32), ("tile_schedule", _i32), ("tune_state", _i32), ("reserved", _i32),
-                ("tune_ns", _d * 6)]
+                ("tile_rows", _i32), ("tile_schedule", _i32), ("tune_state", _i32), ("tune_classes", _i32),
+                ("tune_rounds", _i64), ("tune_hits", _i64), ("tune_ns", _d * 6)]
 
     CANDIDATES = ("8/strided", "8/chunked", "16/strided", "16/chunked", "32/strided", "32/chunked")
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
         d["tune_ns"] = dict(zip(self.CANDIDATES, list(self.tune_ns)))
         d["tile_schedule"] = SCHEDULES.get(self.tile_schedule, self.tile_schedule)
         d["tune_state"] = TUNE_STATES.get(self.tune_state, self.tune_state)

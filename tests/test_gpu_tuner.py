@@ -57,13 +57,14 @@ def test_every_shape_and_the_tuner_give_the_same_bits(sf):
             assert [r["inner_iters"] for r in res] == [r["inner_iters"] for r in res_ref]
             assert same(got, ref), f"{rows}-row {sched} tiles differ from 16-row strided tiles"
     got, res, st = solve(sf, ctx, 0)               # the tuner times every candidate while it solves
-    assert st["tune_state"] == "measured", st
+    assert st["tune_rounds"] >= 1 and st["tune_classes"] >= 1, st
     assert all(v > 0 for v in st["tune_ns"].values())
-    assert f'{st["tile_rows"]}/{st["tile_schedule"]}' == min(st["tune_ns"], key=st["tune_ns"].get)
+    if st["tune_state"] == "measured":
+        assert f'{st["tile_rows"]}/{st["tile_schedule"]}' == min(st["tune_ns"], key=st["tune_ns"].get)
     assert same(got, ref), "the tuned solve differs"
-    chosen = (st["tile_rows"], st["tile_schedule"])
-    got, res, st = solve(sf, ctx, 0)               # same workload class: the context remembers
-    assert st["tune_state"] == "cached" and (st["tile_rows"], st["tile_schedule"]) == chosen
+    classes = st["tune_classes"]
+    got, res, st = solve(sf, ctx, 0)               # the same classes again: the context remembers them
+    assert st["tune_hits"] >= 1 and st["tune_classes"] >= classes, st
     assert same(got, ref)
 
 
