@@ -185,13 +185,14 @@ def run_tune_form(a):
         made = [problem(nx, ny) for nx, ny in sizes]
         sf.solve_stokes_batch_mixed([p for p, _ in made], options=opts, ctx=ctx)
         st = sf.batch_stats(ctx)
-        out[name] = {"chosen": f"{st['tile_rows']} rows {st['tile_schedule']}", "tuner": st["tune_state"],
+        launch = "overlapped" if st["overlap_launches"] else "serial"
+        out[name] = {"chosen": f"{st['tile_rows']}/{st['tile_schedule']}/{launch}", "tuner": st["tune_state"],
                      "grid_points": int(sum((nx - 1) * (ny - 1) for nx, ny in sizes)),
                      "gpts_per_s": {k: round(1.0 / v, 2) for k, v in st["tune_ns"].items() if v > 0}}
         del made
         torch.cuda.empty_cache()
-    return {"form": "tune", "metric": "FP32 sweep throughput per tile shape and schedule, as the engine's tuner "
-                                      "times it", "unit": "G point-sweeps/s", "cases": out,
+    return {"form": "tune", "metric": "FP32 sweep throughput per tile shape, schedule and launch mode, as the "
+                                      "engine's tuner times it", "unit": "G point-sweeps/s", "cases": out,
             "data": "synthetic (smooth random fields, seeded)", "fold_every": a.fold_every, "seed": a.seed}
 
 
@@ -566,7 +567,7 @@ def run_batch_form(a):
     e1.record()
     torch.cuda.synchronize()
     mixed_s = e0.elapsed_time(e1) / 1e3
-    tiles = sf.batch_stats()   # the sweep shape used (the tuner's trial rounds are inside the timed region)
+    tiles = sf.batch_stats()   # the last sweep choice; the tuner's trial pieces are inside the timed region
     e0.record()
     infos = [fp64_solve(d, s) for d, s in zip(inst[:k], fp64_arrs)]
     e1.record()
@@ -607,7 +608,9 @@ def run_batch_form(a):
                                          for f, v in errs.items()},
             "vs_tight_fp64": tight,
             "nonfinite_instances": [q for q, r in enumerate(res) if r["status"] == 5],
-            "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"], "tuner": tiles["tune_state"],
+            "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"],
+                            "overlapped_launches": tiles["overlap_launches"], "tuner": tiles["tune_state"],
+                            "classes_measured": tiles["tune_rounds"], "classes_recalled": tiles["tune_hits"],
                             "gpts_per_s_timed": {k: round(1.0 / v, 2) for k, v in tiles["tune_ns"].items() if v > 0}},
             "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
             "clocks": clk,

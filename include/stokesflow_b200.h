@@ -310,7 +310,8 @@ typedef struct {
                                   autotuner choose the rows and the schedule.  Each round's sweep set has
                                   a workload class (half-octave of the mean, octave of the total grid
                                   points).  The first round of a class the context has not seen begins
-                                  with short timed pieces of every shape and schedule (two each); the
+                                  with short timed pieces of every shape, schedule and launch mode (two
+                                  each); the
                                   fastest per point is then used and recorded in the context, so later
                                   rounds and solves of that class take it at once.  Every shape and
                                   schedule computes the same bits, so the choice changes the speed
@@ -318,6 +319,11 @@ typedef struct {
     int32_t tile_schedule;     /* with tile_rows set: 1 strided (CTA b of G takes tiles b, b+G, ...),
                                   2 chunked (CTA b takes one contiguous run of tiles); 0 = 1.  With
                                   tile_rows 0 it must be 0 (0)                                        */
+    int32_t overlap_launches;  /* with tile_rows set: 1 launches each sweep under programmatic dependent
+                                  launch, so that it starts (and fences its first tensor maps) while the
+                                  previous sweep drains; 0 serialises the launches.  With tile_rows 0
+                                  the tuner chooses, and it must be 0 (0)                             */
+    int32_t reserved;          /* 0 */
 } sf_mixed_options;
 
 /* sf_engine_stats.tune_state */
@@ -376,12 +382,15 @@ typedef struct {
     int32_t pending_results;   /* finished, not yet reported by sf_engine_step   */
     int32_t tile_rows;         /* rows of the sweep tiles in use                 */
     int32_t tile_schedule;     /* 1 strided, 2 chunked                           */
+    int32_t overlap_launches;  /* 1: sweeps launched overlapped                  */
     int32_t tune_state;        /* SF_TUNE_* for the current workload class       */
     int32_t tune_classes;      /* workload classes with a recorded choice in the context */
+    int32_t reserved;
     int64_t tune_rounds;       /* rounds whose sweeps began with timed trial pieces */
     int64_t tune_hits;         /* workload-class changes answered from the context's record */
-    double tune_ns[6];         /* the last completed measurement: ns per point-sweep of 8 rows strided,
-                                  8 chunked, 16 strided, 16 chunked, 32 strided, 32 chunked (0: none) */
+    double tune_ns[12];        /* the last completed measurement: ns per point-sweep of each candidate,
+                                  (rows, schedule, launch) in the order 8 strided serialised, 8 strided
+                                  overlapped, 8 chunked serialised, ..., 32 chunked overlapped (0: none) */
 } sf_engine_stats;
 
 /* Arena bytes one instance of Nx x Ny grid points holds while admitted. */

@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <map>
+#include <utility>
 #include <string>
 
 #include "stokesflow_b200.h"
@@ -100,6 +101,25 @@ bool distinct_contexts(int n, Get get) {
     return true;
 }
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// launches `kern`; with `overlap`, under programmatic stream serialization: it may begin (launch, prologue)
+// while the previous kernel on `s` drains, and must call griddep_wait() before it touches that kernel's
+// results (sf_tma.cuh)
+template <typename... Params, typename... Args>
+cudaError_t launch_overlapped(bool overlap, void (*kern)(Params...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, Args&&... args) {
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = overlap ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }

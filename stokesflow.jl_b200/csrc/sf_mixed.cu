@@ -120,14 +120,39 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
     const int ntiles = *ntiles_ptr;
+    // schedule: strided (CTA b of G takes tiles b, b + G, ...: neighbouring tiles run side by side) or chunked
+    // (CTA b takes a contiguous run of ceil(ntiles / G) tiles: it meets few instances, so it fences few maps)
+    const int G = gridDim.x;
+    int first, step, end;
+    if (chunked) {
+        const int chunk = (ntiles + G - 1) / G;
+        first = blockIdx.x * chunk;
+        step = 1;
+        end = min(ntiles, first + chunk);
+    } else {
+        first = blockIdx.x;
+        step = G;
+        end = ntiles;
+    }
+    // the tile list is ordered by instance, so a CTA meets each instance in one run of tiles: the two maps it
+    // reads are fenced when the run starts
+    int fenced = -1;
+    auto fence_maps = [&](int x) {
+        fence_tensormap_acquire(maps + (int64_t)x * M_NUM + M_HALO);
+        fence_tensormap_acquire(maps + (int64_t)x * M_NUM + M_TILE);
+        fenced = x;
+    };
     if (tid == 0) {
         for (int k = 0; k < NST; ++k) mbar_init(&bar[k], 1);
         fence_mbar_init();
+        // the first instance's maps are fenced before the wait below, while the previous sweep may still run:
+        // maps, tile list and tile count are written by host copies before the sweeps, never by a sweep
+        if (first < end) fence_maps(tiles[first].x);
     }
     __syncthreads();
-    // the tile list is ordered by instance, so a CTA meets each instance in one run of tiles: the maps it
-    // reads are fenced when the run starts
-    int fenced = -1;
+    // the previous sweep's corrections and rates are complete and visible from here on
+    griddep_wait();
+    griddep_launch_dependents();
     auto issue = [&](int t, int s) {  // thread 0 only
         const int2 td = tiles[t];
         const Inst& I = insts[td.x];
@@ -135,11 +160,7 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         const int in = (I.parity ^ launch_parity) & 1;
         const CUtensorMap* H = maps + (int64_t)td.x * M_NUM + M_HALO;
         const CUtensorMap* T = maps + (int64_t)td.x * M_NUM + M_TILE;
-        if (td.x != fenced) {
-            fence_tensormap_acquire(H);
-            fence_tensormap_acquire(T);
-            fenced = td.x;
-        }
+        if (td.x != fenced) fence_maps(td.x);
         unsigned char* st = smem + s * STAGE_BYTES;
         mbar_arrive_expect_tx(&bar[s], STAGE_TX);
         tma_load_3d(st + 0 * HALO_BYTES, H, &bar[s], i0, j0, in ? G_VXB : G_VXA);
@@ -155,20 +176,6 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         tma_load_3d(tb + 2 * TILE_BYTES, T, &bar[s], i0, j0, G_RX);
         tma_load_3d(tb + 3 * TILE_BYTES, T, &bar[s], i0, j0, G_RY);
     };
-    // schedule: strided (CTA b takes tiles b, b + G, ...: neighbouring tiles run side by side) or chunked (CTA b
-    // takes a contiguous run of ceil(ntiles / G) tiles: it meets few instances, so it fences few maps)
-    const int G = gridDim.x;
-    int first, step, end;
-    if (chunked) {
-        const int chunk = (ntiles + G - 1) / G;
-        first = blockIdx.x * chunk;
-        step = 1;
-        end = min(ntiles, first + chunk);
-    } else {
-        first = blockIdx.x;
-        step = G;
-        end = ntiles;
-    }
     int t = first;
     if (tid == 0)
         for (int k = 0; k < NST - 1; ++k)
@@ -623,11 +630,15 @@ static const SweepShape kShapes[] = {
 constexpr int NSHAPES = (int)(sizeof(kShapes) / sizeof(kShapes[0]));
 // tile schedules of the persistent sweep kernel: 0 strided, 1 chunked (the kernel's `chunked` argument)
 constexpr int NSCHED = 2;
-// the tuner's candidates: shape k with schedule c is candidate k * NSCHED + c
-constexpr int NCAND = NSHAPES * NSCHED;
-static_assert(NCAND == 6, "sf_engine_stats.tune_ns has one entry per candidate");
+// sweep launches: 0 serialised, 1 overlapped (programmatic dependent launch: a sweep launches and fences its
+// first maps while the previous one drains, and waits in the kernel for its results)
+constexpr int NLAUNCH = 2;
+// the tuner's candidates: shape k, schedule c, launch mode o is candidate (k * NSCHED + c) * NLAUNCH + o
+constexpr int NCAND = NSHAPES * NSCHED * NLAUNCH;
+static_assert(NCAND == 12, "sf_engine_stats.tune_ns has one entry per candidate");
+constexpr int cand_of(int k, int c, int o) { return (k * NSCHED + c) * NLAUNCH + o; }
 constexpr int DEFAULT_SHAPE = 1;                      // 32 x 16 rows ...
-constexpr int DEFAULT_CAND = DEFAULT_SHAPE * NSCHED + 1;  // ... chunked, until measured otherwise
+constexpr int DEFAULT_CAND = cand_of(DEFAULT_SHAPE, 1, 0);  // ... chunked, serialised, until measured
 constexpr int TUNE_PASSES = 2;                        // timed pieces per candidate; the fastest counts
 
 static int shape_of_rows(int rows) {
@@ -737,6 +748,7 @@ static sf_mixed_options normalized(const sf_mixed_options* o) {
         r.retry_local_max = 1;
         r.tile_rows = 0;
         r.tile_schedule = 0;
+        r.overlap_launches = 0;
     }
     if (r.fold_every < 2) r.fold_every = 2;
     r.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
@@ -789,6 +801,7 @@ struct sf_engine {
     // timed on the engine stream; the shape with the fewest ns per point-sweep is kept and recorded in the context
     int shape = DEFAULT_SHAPE;
     int sched = 0;
+    int overlap = 0;
     int tune_state = SF_TUNE_MEASURING;
     int tune_trials = 0;
     int tune_key = -1;
@@ -921,7 +934,7 @@ int upload_sweep_list(sf_engine* e, const std::vector<int>& ids, int k) {
     int64_t nt = 0;
     for (int q : ids) nt += e->slots[q].ntiles[k];
     if (nt > e->tile_cap[k])  // the shape's graphs hold the old pointer
-        for (int c = 0; c < NSCHED; ++c) drop_graph(e, k * NSCHED + c);
+        for (int c = cand_of(k, 0, 0); c < cand_of(k + 1, 0, 0); ++c) drop_graph(e, c);
     int rc = grow_list(e, nt, &e->d_tiles[k], nullptr, &e->tile_cap[k]);
     if (rc) return rc;
     std::vector<int2>& h = e->h_list[k];
@@ -953,8 +966,11 @@ int encode_maps(sf_engine* e, int q) {
     return SF_OK;
 }
 
-// switches the sweeps to shape k with schedule c (persistent grid size; the maps and lists are per shape)
-int use_shape(sf_engine* e, int k, int c) {
+// switches the sweeps to a candidate: its shape k (persistent grid size; the maps and lists are per shape),
+// schedule and launch mode
+int use_cand(sf_engine* e, int cand) {
+    const int k = cand / (NSCHED * NLAUNCH), c = (cand / NLAUNCH) % NSCHED;
+    e->overlap = cand % NLAUNCH;
     int per_sm = 0;
     int rc = shape_per_sm(e->ctx->device, k, &per_sm);
     if (rc) return rc;
@@ -967,16 +983,18 @@ int use_shape(sf_engine* e, int k, int c) {
 
 // the caller's tile_rows (and tile_schedule) fix the sweeps; tile_rows 0 lets the tuner choose both
 int configure_tuner(sf_engine* e) {
-    int k = DEFAULT_CAND / NSCHED, c = DEFAULT_CAND % NSCHED;
-    const int sc = e->opt.tile_schedule;
+    int cand = DEFAULT_CAND;
+    const int sc = e->opt.tile_schedule, ov = e->opt.overlap_launches;
     if (e->opt.tile_rows != 0) {
-        k = shape_of_rows(e->opt.tile_rows);
+        const int k = shape_of_rows(e->opt.tile_rows);
         if (k < 0) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_rows must be 0, 8, 16 or 32");
         if (sc < 0 || sc > NSCHED) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_schedule must be 0, 1 or 2");
-        c = sc == 2 ? 1 : 0;
+        if (ov < 0 || ov > 1) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.overlap_launches must be 0 or 1");
+        cand = cand_of(k, sc == 2 ? 1 : 0, ov);
         e->tune_state = SF_TUNE_FIXED;
     } else {
-        if (sc != 0) return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_schedule needs tile_rows");
+        if (sc != 0 || ov != 0)
+            return fail(SF_ERR_INVALID_ARG, "sf_mixed_options.tile_schedule and overlap_launches need tile_rows");
         e->tune_state = SF_TUNE_MEASURING;
     }
     e->tune_trials = 0;
@@ -985,7 +1003,7 @@ int configure_tuner(sf_engine* e) {
     e->tune_rounds = e->tune_hits = 0;
     for (double& v : e->tune_ns) v = 0.0;
     for (double& v : e->trial_ns) v = 0.0;
-    return use_shape(e, k, c);
+    return use_cand(e, cand);
 }
 
 // workload class of a sweep set: half-octaves of the mean points per instance, octaves of the total points
@@ -1018,18 +1036,18 @@ int tuner_collect(sf_engine* e) {
     for (int k = 0; k < NCAND; ++k) e->tune_ns[k] = e->trial_ns[k];
     e->tune_state = SF_TUNE_MEASURED;
     e->ctx->sweep_shapes[e->tune_key] = best;
-    return use_shape(e, best / NSCHED, best % NSCHED);
+    return use_cand(e, best);
 }
 
 // `n` sweeps (launch parities k0, k0 + 1, ...) over the uploaded sweep list of the current shape
 int launch_direct(sf_engine* e, int k0, int n) {
     const int sk = e->shape;
     const SweepShape& sh = kShapes[sk];
-    for (int k = k0; k < k0 + n; ++k) {
-        sh.kern<<<e->blocks, dim3(BX, TY), sh.smem, e->s>>>(maps_of(e, sk), e->d_insts, e->d_tiles[sk],
-                                                             e->d_ntiles + sk, k & 1, e->sched, e->d_flag);
-        SF_CHECK_LAUNCH();
-    }
+    // overlapped: each sweep may launch while the previous one drains; it waits in the kernel for its results
+    for (int k = k0; k < k0 + n; ++k)
+        SF_CUDA(launch_overlapped(e->overlap != 0, sh.kern, dim3(e->blocks), dim3(BX, TY), (size_t)sh.smem, e->s,
+                                  maps_of(e, sk), (const Inst*)e->d_insts, (const int2*)e->d_tiles[sk],
+                                  (const int*)(e->d_ntiles + sk), k & 1, e->sched, e->d_flag));
     return SF_OK;
 }
 
@@ -1040,7 +1058,7 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     const int K = e->opt.fold_every;
     const int P = std::min(8, std::max(2, (K / (2 * NCAND)) & ~1));
     const int pieces = std::min(NCAND * TUNE_PASSES - e->tune_trials, K / P);
-    const int prev_shape = e->shape, prev_sched = e->sched;
+    const int prev = cand_of(e->shape, e->sched, e->overlap);
     int rc, k = 0;
     ++e->tune_rounds;
     for (int sk = 0; sk < NSHAPES; ++sk)
@@ -1048,7 +1066,7 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     SF_CUDA(cudaEventRecord(e->ev_piece[0], e->s));
     for (int i = 0; i < pieces; ++i, k += P) {
         const int cand = (e->tune_trials + i) % NCAND;
-        if ((rc = use_shape(e, cand / NSCHED, cand % NSCHED))) return rc;
+        if ((rc = use_cand(e, cand))) return rc;
         if ((rc = launch_direct(e, k, P))) return rc;
         SF_CUDA(cudaEventRecord(e->ev_piece[i + 1], e->s));
     }
@@ -1056,7 +1074,7 @@ int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     e->timed_pieces = pieces;
     e->timed_points = points * P;
     if (k < K) {  // the rest in the choice made before (the previous class's, or the default)
-        if ((rc = use_shape(e, prev_shape, prev_sched))) return rc;
+        if ((rc = use_cand(e, prev))) return rc;
         if ((rc = launch_direct(e, k, K - k))) return rc;
     }
     return SF_OK;
@@ -1079,7 +1097,7 @@ int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
             if (it != e->ctx->sweep_shapes.end()) {
                 e->tune_state = SF_TUNE_CACHED;
                 ++e->tune_hits;
-                if ((rc = use_shape(e, it->second / NSCHED, it->second % NSCHED))) return rc;
+                if ((rc = use_cand(e, it->second))) return rc;
             } else {
                 e->tune_state = SF_TUNE_MEASURING;
             }
@@ -1093,7 +1111,7 @@ int launch_sweeps(sf_engine* e, const std::vector<int>& ids) {
     }
     if ((rc = upload_sweep_list(e, ids, e->shape))) return rc;
     if (e->opt.use_graphs) {
-        const int c = e->shape * NSCHED + e->sched;
+        const int c = cand_of(e->shape, e->sched, e->overlap);
         if (e->gexec[c] && e->graph_k[c] != K) drop_graph(e, c);
         if (!e->gexec[c]) {
             SF_CUDA(cudaStreamBeginCapture(e->s, cudaStreamCaptureModeThreadLocal));
@@ -1423,6 +1441,7 @@ extern "C" int sf_engine_get_stats(sf_engine* e, sf_engine_stats* st) {
     st->pending_results = (int32_t)e->pending.size();
     st->tile_rows = kShapes[e->shape].rows;
     st->tile_schedule = e->sched + 1;
+    st->overlap_launches = e->overlap;
     st->tune_state = e->tune_state;
     st->tune_classes = (int32_t)e->ctx->sweep_shapes.size();
     st->tune_rounds = e->tune_rounds;

@@ -25,6 +25,14 @@ __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream serialization may start while
+// the previous kernel in the stream is still running; griddep_wait() returns once that kernel has completed
+// and its memory operations are visible, so nothing it writes may be read (or overwritten) before it.
+// griddep_launch_dependents() lets the next such kernel start its own launch and prologue.  Both are no-ops
+// for a kernel launched without the attribute.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");

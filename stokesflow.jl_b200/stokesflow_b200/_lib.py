@@ -76,20 +76,24 @@ class BatchInstance(C.Structure):
 class MixedOptions(C.Structure):
     """sf_mixed_options."""
     _fields_ = [("max_sweeps", _i64), ("fold_every", _i32), ("use_graphs", _i32), ("dtau_local_max", _i32),
-                ("retry_local_max", _i32), ("tile_rows", _i32), ("tile_schedule", _i32)]
+                ("retry_local_max", _i32), ("tile_rows", _i32), ("tile_schedule", _i32), ("overlap_launches", _i32),
+                ("reserved", _i32)]
 
 
 class EngineStats(C.Structure):
     """sf_engine_stats."""
     _fields_ = [("arena_bytes", _i64), ("arena_used", _i64), ("arena_peak", _i64), ("submitted", _i64),
                 ("finished", _i64), ("rounds", _i64), ("sweeps", _i64), ("active", _i32), ("pending_results", _i32),
-                ("tile_rows", _i32), ("tile_schedule", _i32), ("tune_state", _i32), ("tune_classes", _i32),
-                ("tune_rounds", _i64), ("tune_hits", _i64), ("tune_ns", _d * 6)]
+                ("tile_rows", _i32), ("tile_schedule", _i32), ("overlap_launches", _i32), ("tune_state", _i32),
+                ("tune_classes", _i32), ("reserved", _i32), ("tune_rounds", _i64), ("tune_hits", _i64),
+                ("tune_ns", _d * 12)]
 
-    CANDIDATES = ("8/strided", "8/chunked", "16/strided", "16/chunked", "32/strided", "32/chunked")
+    # rows/schedule/launch, in the library's candidate order
+    CANDIDATES = tuple(f"{r}/{c}/{o}" for r in (8, 16, 32) for c in ("strided", "chunked")
+                       for o in ("serial", "overlapped"))
 
     def as_dict(self):
-        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
         d["tune_ns"] = dict(zip(self.CANDIDATES, list(self.tune_ns)))
         d["tile_schedule"] = SCHEDULES.get(self.tile_schedule, self.tile_schedule)
         d["tune_state"] = TUNE_STATES.get(self.tune_state, self.tune_state)

@@ -231,16 +231,17 @@ class MixedProblem:
 
 
 def mixed_options(max_sweeps=4_000_000, fold_every=400, use_graphs=True, dtau_local_max=False,
-                  retry_local_max=True, tile_rows=0, tile_schedule=None):
+                  retry_local_max=True, tile_rows=0, tile_schedule=None, overlap_launches=False):
     """Options of the mixed-precision / batched solver (sf_mixed_options).  dtau_local_max: pseudo-time
     steps from the stencil's largest viscosity instead of the reference's average (faster on soft
     inclusions); the converged solution is the same.  retry_local_max: an instance that diverges restarts
     from its inputs with the stencil-maximum step.  tile_rows: 8, 16 or 32 rows per sweep tile, or 0 for
-    the autotuner's choice of rows and schedule (every choice gives the same bits); tile_schedule
-    ("strided" or "chunked") goes with a fixed tile_rows."""
+    the autotuner's choice of rows, schedule and launch mode (every choice gives the same bits);
+    tile_schedule ("strided" or "chunked") and overlap_launches (sweeps launched under programmatic dependent
+    launch) go with a fixed tile_rows."""
     sched = {None: 0, "strided": 1, "chunked": 2}[tile_schedule]
     return _lib.MixedOptions(int(max_sweeps), int(fold_every), int(bool(use_graphs)), int(bool(dtau_local_max)),
-                             int(bool(retry_local_max)), int(tile_rows), sched)
+                             int(bool(retry_local_max)), int(tile_rows), sched, int(bool(overlap_launches)), 0)
 
 
 def batch_stats(ctx: Context | None = None) -> dict:

@@ -54,6 +54,35 @@ def test_library_is_sm100a_build():
     assert b"sm_100a" in so or b"compute_100a" in so
 
 
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every struct of the C ABI has the size and field offsets of its ctypes mirror (a C program compiled
+    against include/stokesflow_b200.h prints them)."""
+    mirrors = {}
+    for cls in vars(_lib).values():
+        if isinstance(cls, type) and issubclass(cls, C.Structure) and cls.__doc__:
+            m = re.match(r"(sf_[a-z_]+)\.", cls.__doc__.strip())
+            if m:
+                mirrors[m.group(1)] = cls
+    assert len(mirrors) >= 9
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "stokesflow_b200.h"', "int main(void) {"]
+    for name, cls in mirrors.items():
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for f, _ in cls._fields_:
+            lines.append(f'printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    import subprocess
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                        text=True).stdout.splitlines())
+    for name, cls in mirrors.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for f, _ in cls._fields_:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, f"{name}.{f}"
+
+
 def test_status_strings(L):
     assert L.sf_status_string(0) == b"ok"
     assert L.sf_status_string(_lib.SF_ERR_NONFINITE) == b"non-finite residual"

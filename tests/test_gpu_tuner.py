@@ -22,7 +22,7 @@ def specs():
     return out
 
 
-def solve(sf, ctx, tile_rows, fold_every=50, schedule=None):
+def solve(sf, ctx, tile_rows, fold_every=50, schedule=None, overlap=False):
     import torch
     probs, arrs = [], []
     for (Nx, Ny, dx, dy, (rho, mub, mup)) in specs():
@@ -33,7 +33,8 @@ def solve(sf, ctx, tile_rows, fold_every=50, schedule=None):
         arrs.append(a)
         probs.append(sf.MixedProblem(a["P"], a["Vx_pad"], a["Vy_pad"], a["rho_vy"], a["mu_b"], a["mu_p"],
                                      a["Vx_s"], a["Vy_s"], 9.81, dx, dy, Nx, Ny, 0.0, 0.5, rel_tol=1e-8))
-    opts = sf.mixed_options(fold_every=fold_every, tile_rows=tile_rows, tile_schedule=schedule)
+    opts = sf.mixed_options(fold_every=fold_every, tile_rows=tile_rows, tile_schedule=schedule,
+                            overlap_launches=overlap)
     res = sf.solve_stokes_batch_mixed(probs, options=opts, ctx=ctx)
     out = [{k: a[k].cpu().numpy() for k in ("P", "Vx_pad", "Vy_pad")} for a in arrs]
     return out, res, sf.batch_stats(ctx)
@@ -43,6 +44,10 @@ def same(a, b):
     return all(np.array_equal(x[k], y[k]) for x, y in zip(a, b) for k in x)
 
 
+def chosen(st):
+    return f'{st["tile_rows"]}/{st["tile_schedule"]}/{"overlapped" if st["overlap_launches"] else "serial"}'
+
+
 def test_every_shape_and_the_tuner_give_the_same_bits(sf):
     ctx = sf.Context(0)
     ref, res_ref, st = solve(sf, ctx, 16)
@@ -50,17 +55,18 @@ def test_every_shape_and_the_tuner_give_the_same_bits(sf):
     assert all(r["converged"] == 1 for r in res_ref)
     for rows in (8, 16, 32):
         for sched in ("strided", "chunked"):
-            if (rows, sched) == (16, "strided"):
-                continue
-            got, res, st = solve(sf, ctx, rows, schedule=sched)
-            assert (st["tile_rows"], st["tile_schedule"]) == (rows, sched)
-            assert [r["inner_iters"] for r in res] == [r["inner_iters"] for r in res_ref]
-            assert same(got, ref), f"{rows}-row {sched} tiles differ from 16-row strided tiles"
+            for overlap in (False, True):
+                if (rows, sched, overlap) == (16, "strided", False):
+                    continue
+                got, res, st = solve(sf, ctx, rows, schedule=sched, overlap=overlap)
+                assert (st["tile_rows"], st["tile_schedule"], st["overlap_launches"]) == (rows, sched, int(overlap))
+                assert [r["inner_iters"] for r in res] == [r["inner_iters"] for r in res_ref]
+                assert same(got, ref), f"{rows}-row {sched} tiles (overlapped {overlap}) differ from the reference run"
     got, res, st = solve(sf, ctx, 0)               # the tuner times every candidate while it solves
     assert st["tune_rounds"] >= 1 and st["tune_classes"] >= 1, st
     assert all(v > 0 for v in st["tune_ns"].values())
     if st["tune_state"] == "measured":
-        assert f'{st["tile_rows"]}/{st["tile_schedule"]}' == min(st["tune_ns"], key=st["tune_ns"].get)
+        assert chosen(st) == min(st["tune_ns"], key=st["tune_ns"].get)
     assert same(got, ref), "the tuned solve differs"
     classes = st["tune_classes"]
     got, res, st = solve(sf, ctx, 0)               # the same classes again: the context remembers them
@@ -71,10 +77,11 @@ def test_every_shape_and_the_tuner_give_the_same_bits(sf):
 def test_bad_tile_options_rejected(sf):
     with pytest.raises(StokesFlowError):
         solve(sf, sf.Context(0), 12)
-    bad = sf.mixed_options()
-    bad.tile_schedule = 2                          # a schedule without a fixed shape
-    with pytest.raises(StokesFlowError):
-        sf.Engine(arena_bytes=64 << 20, options=bad)
+    for field in ("tile_schedule", "overlap_launches"):   # without a fixed shape
+        bad = sf.mixed_options()
+        setattr(bad, field, 1)
+        with pytest.raises(StokesFlowError):
+            sf.Engine(arena_bytes=64 << 20, options=bad)
 
 
 def test_engine_reports_its_shape(sf):
