@@ -44,7 +44,7 @@ METRIC = "PT T_eff (essential HBM bytes of the PT iterations / time), FP64, rela
 UNIT = "GB/s"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
-TRAFFIC_PER_LAUNCH_2048 = 470.756e6   # dram__bytes_read.sum + dram__bytes_write.sum, k_pt_iter, 2047^2 points
+TRAFFIC_PER_LAUNCH_2048 = 402.079e6   # dram__bytes_read.sum + dram__bytes_write.sum, k_pt_iter, 2047^2 points
 
 
 # ---------------------------------------------------------------------------

@@ -7,7 +7,7 @@
 //
 //   * the domain is cut into BX x BY tiles of points (i, j), 0 <= i < Nx-1,
 //     0 <= j < Ny-1 (the pressure index space, which contains the dVx and dVy
-//     index spaces); persistent CTAs (3 per SM) walk the tiles;
+//     index spaces); persistent CTAs (4 per SM) walk the tiles;
 //   * one thread per CTA brings the next tile's old Vx, Vy, rho, P, mu_p, mu_b
 //     (tile + 2 halo) and dVx, dVy (tile) into a second shared-memory stage
 //     with bulk-tensor copies (TMA, mbarrier-completed) while the CTA computes
@@ -17,16 +17,18 @@
 //     than a grid-wide barrier), then the residuals, the damped rates dV and
 //     the new velocities of its tile;
 //   * tau and divV are stored only on check iterations; dtauVx, dtauVy are
-//     computed once per solve, as compute_timesteps! does, and streamed in
-//     with the tile (16 B per point instead of 4 FP64 divisions);
+//     computed in the kernel from the staged mu_p with compute_timesteps!'s
+//     expression (4 FP64 divisions per point cost less than streaming two
+//     precomputed arrays, 16 B per point, and free the shared memory for a
+//     fourth CTA per SM);
 //   * the free-slip ghost rows / columns of the new velocities are written by
 //     the CTAs on the domain edge, in the reference's BC order (:53-56);
 //   * V and P are double-buffered (the iteration is Jacobi-like: every read is
 //     an old value), dV is updated in place.
 //
 // HBM bytes per iteration: read Vx, Vy, P, dVx, dVy, rho, mu_b, mu_p and write
-// Vx, Vy, P, dVx, dVy -- 13 arrays, ~104 * Nx * Ny bytes essential, plus the
-// two dtau arrays read (16 * Nx * Ny).
+// Vx, Vy, P, dVx, dVy -- 13 arrays, ~104 * Nx * Ny bytes, which is all the
+// kernel reads and writes.
 //
 // Fields live in a padded internal layout (one leading dimension LD, a
 // multiple of 32 doubles, for every field) packed from / unpacked to the
@@ -52,7 +54,7 @@ namespace sf {
 
 enum {
     F_VXA, F_VXB, F_VYA, F_VYB, F_PA, F_PB, F_DVX, F_DVY, F_RHO, F_MUB, F_MUP,
-    F_TXX, F_TYY, F_TXY, F_DIV, F_RX, F_RY, F_DTVX, F_DTVY, F_NUM
+    F_TXX, F_TYY, F_TXY, F_DIV, F_RX, F_RY, F_NUM
 };
 
 struct Layout {
@@ -99,8 +101,8 @@ struct PTParams {
 // overlap the arithmetic without needing high occupancy.  A stage holds the
 // old Vx, Vy, rho_vy, P, mu_p, mu_b boxes (tile + 2 halo; the TMA zero-fills
 // beyond the arrays) and the dVx, dVy boxes (tile only).
-// 32 x 8 tiles: 60 KB of shared memory per CTA, 3 CTAs per SM (32 x 16 allowed 2; same speed at 2048^2,
-// 10% faster at 4096^2)
+// 32 x 8 tiles: 51 KB of shared memory per CTA, 4 CTAs per SM (32 x 16 tiles allowed 2 before the dtau
+// arrays left the stage: same speed at 2048^2, 10% slower at 4096^2)
 #ifndef SF_PT_BY
 #define SF_PT_BY 8
 #endif
@@ -115,22 +117,22 @@ constexpr int NST = SF_PT_STAGES;                      // shared-memory stages (
 static_assert(NST >= 2 && NST <= 8, "2..8 pipeline stages");
 static_assert(BY % TY == 0, "tile rows must be a multiple of the thread rows");
 constexpr int PT_THREADS = BX * TY;
-constexpr int PT_MIN_BLOCKS = (PT_THREADS >= 512) ? 2 : 3;
+constexpr int PT_MIN_BLOCKS = (PT_THREADS >= 512) ? 2 : 4;
 constexpr int TW = BX + 2, TH = BY + 2;      // staged box (tile + 2 halo); TW*8 is a multiple of 16 bytes
 constexpr int W1 = BX + 1, H1 = BY + 1;      // P / tau points computed per tile (tile + 1 halo)
 constexpr int RPT = BY / TY;                 // owned rows per thread
 constexpr int ARR_BYTES = ((TH * TW * 8 + 127) / 128) * 128;
 constexpr int DV_BYTES = ((BY * BX * 8 + 127) / 128) * 128;
 constexpr int ST1_BYTES = ((H1 * W1 * 8 + 127) / 128) * 128;
-constexpr int STAGE_BYTES = 6 * ARR_BYTES + 4 * DV_BYTES;         // + dVx, dVy, dtauVx, dtauVy boxes
-constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 4 * BY * BX * 8;  // bytes delivered per stage
+constexpr int STAGE_BYTES = 6 * ARR_BYTES + 2 * DV_BYTES;         // + dVx, dVy boxes
+constexpr uint32_t STAGE_TX = 6 * TH * TW * 8 + 2 * BY * BX * 8;  // bytes delivered per stage
 constexpr int SMEM_BYTES = NST * STAGE_BYTES + 4 * ST1_BYTES + 64;
 constexpr uint64_t WAIT_BUDGET_NS = 2000000000ull;                 // 2 s per stage wait
 enum { S_VX = 0, S_VY, S_RHO, S_P, S_MUP, S_MUB };
 
 struct TmaMaps {
     CUtensorMap f[6];  // S_* order
-    CUtensorMap dvx, dvy, dtx, dty;
+    CUtensorMap dvx, dvy;
 };
 
 template <bool STORE>
@@ -164,8 +166,6 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         for (int k = 0; k < 6; ++k) tma_load_2d(st + k * ARR_BYTES, &maps.f[k], &bar[s], i0, j0);
         tma_load_2d(st + 6 * ARR_BYTES, &maps.dvx, &bar[s], i0, j0);
         tma_load_2d(st + 6 * ARR_BYTES + DV_BYTES, &maps.dvy, &bar[s], i0, j0);
-        tma_load_2d(st + 6 * ARR_BYTES + 2 * DV_BYTES, &maps.dtx, &bar[s], i0, j0);
-        tma_load_2d(st + 6 * ARR_BYTES + 3 * DV_BYTES, &maps.dty, &bar[s], i0, j0);
     };
     const int G = gridDim.x;
     int t = blockIdx.x;
@@ -194,8 +194,6 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
         Row2* sMub = reinterpret_cast<Row2*>(st + S_MUB * ARR_BYTES);
         RowD* sDvx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES);
         RowD* sDvy = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + DV_BYTES);
-        RowD* sDtx = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 2 * DV_BYTES);  // dtauVx of :129
-        RowD* sDty = reinterpret_cast<RowD*>(st + 6 * ARR_BYTES + 3 * DV_BYTES);  // dtauVy of :130
         const int i0 = (t % p.ntx) * BX, j0 = (t / p.ntx) * BY;
         // interior tiles: every point of the tile and its halo is inside, no boundary node among them
         const bool interior = i0 > 0 && j0 > 0 && i0 + BX + 2 < Nx && j0 + BY + 2 < Ny;
@@ -269,7 +267,8 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
                         - (sPn[b][a + 1] - sPn[b][a]) * _dx;
             double dv = p.dampX * sDvx[b][a] + Rx;
             dVx_t[o] = dv;
-            return sVx[b + 1][a + 1] + sDtx[b][a] * dv;
+            const double dtau = p.c_vsc / ((sMup[b][a] + sMup[b][a + 1]) * 0.5) / 4.1;  // dtauVx (:129)
+            return sVx[b + 1][a + 1] + dtau * dv;
         };
         auto new_vy = [&](int a, int b, int o) {
             // compute_ResY (:189-202)
@@ -282,7 +281,8 @@ __global__ void __launch_bounds__(PT_THREADS, PT_MIN_BLOCKS) k_pt_iter(const __g
                                                                + sVy[b + 1][a + 1] * d_yi_2_rho * 0.5 * _dy));
             double dv = p.dampY * sDvy[b][a] + Ry;
             dVy_t[o] = dv;
-            return sVy[b + 1][a + 1] + sDty[b][a] * dv;
+            const double dtau = p.c_vsc / ((sMup[b][a] + sMup[b + 1][a]) * 0.5) / 4.1;  // dtauVy (:130)
+            return sVy[b + 1][a + 1] + dtau * dv;
         };
         if (interior) {
 #pragma unroll
@@ -648,8 +648,6 @@ struct Solver {
             }
             int rc = encode_tmap_f64(&maps[c].dvx, L.f(F_DVX), LD, R, BX, BY);
             if (!rc) rc = encode_tmap_f64(&maps[c].dvy, L.f(F_DVY), LD, R, BX, BY);
-            if (!rc) rc = encode_tmap_f64(&maps[c].dtx, L.f(F_DTVX), LD, R, BX, BY);
-            if (!rc) rc = encode_tmap_f64(&maps[c].dty, L.f(F_DTVY), LD, R, BX, BY);
             if (rc) return rc;
         }
         static bool attr_set = false;
@@ -765,13 +763,8 @@ static int solver_prepare(Solver& S, sf_ctx* ctx, cudaStream_t s, const SolveArg
     }
     k_set_scalar<<<1, 1, 0, s>>>(ctx->d_scalars + SC_DT, dt);
     SF_LAUNCHED(ctx);
-    // compute_timesteps! (:34): dtauVx, dtauVy once per solve into the padded layout (the fused
-    // kernel reads them instead of dividing every iteration); also into the caller's arrays if given
-    k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
-                                                                     Vsc * min_dxy2, Ptsc * 4.1, max_nxy,
-                                                                     S.L.f(F_DTVX), LD, S.L.f(F_DTVY), LD,
-                                                                     nullptr, 0);
-    SF_LAUNCHED(ctx);
+    // compute_timesteps! (:34) into the caller's work arrays, if given; the fused kernel computes the same
+    // pseudo-time steps from the staged mu_p as it needs them
     if (A.dtVx || A.dtVy || A.dtPt) {
         k_timesteps<<<copy_blocks(ctx, (Nx - 1) * (Ny - 1)), 256, 0, s>>>(S.L.f(F_MUP), LD, (int)Nx, (int)Ny,
                                                                          Vsc * min_dxy2, Ptsc * 4.1, max_nxy,
