@@ -18,11 +18,14 @@
 //   3. FP64 fold: V_{k+1} = V_k + dV, P_{k+1} = P_k + dP; back to 1.
 //
 // All instances live in one arena.  Every FP32 sweep is ONE persistent kernel
-// launch over a device-resident work list of 32 x 16 tiles from all instances
-// in their inner phase, with per-instance tensor maps (TMA, double-buffered,
-// no multicast) -- so hundreds of small problems cost one launch per
-// iteration instead of hundreds.  The runs of iterations between checks are
-// replayed from a captured CUDA graph.  Instances move between phases
+// launch over a device-resident work list of 32-column tiles from all
+// instances in their inner phase, with per-instance tensor maps (TMA,
+// double-buffered, no multicast) -- so hundreds of small problems cost one
+// launch per iteration instead of hundreds.  The runs of iterations between
+// checks are replayed from captured CUDA graphs.  The tile rows (8, 16, 32),
+// the order in which the CTAs take the tiles and whether consecutive sweeps
+// overlap their launches are chosen per workload class by timing them (the
+// tuner); every choice computes the same bits.  Instances move between phases
 // independently, which is what lets a serving loop add and retire instances
 // while others run.
 //
