@@ -72,11 +72,14 @@ void orc_marker_counts(int64_t marker_density, int64_t nx, int64_t ny, int64_t* 
     *nmy = marker_density * (ny - 1);
 }
 
-/* Julia LinRange(a, b, n)[k] = lerpi(k-1, n-1, a, b) = fma(t, b, fma(-t, a, a)), t=(k-1)/(n-1) */
+/* Julia LinRange(a, b, n)[k] = lerpi(k-1, n-1, a, b) = (1 - t)*a + t*b, t = (k-1)/(n-1): two products and a
+ * sum, each rounded.  That is the form the reference's golden values fit: the fma form of lerpi,
+ * fma(t, b, fma(-t, a, a)), differs in the last bit and puts a marker of the 5-timestep golden case
+ * (test/test_StokesFlow2D.jl) on the other side of the plume boundary */
 static double linrange_at(double a, double b, int64_t n, int64_t k) {
     if (n == 1) return a;
     double t = (double)(k - 1) / (double)(n - 1);
-    return fma(t, b, fma(-t, a, a));
+    return (1.0 - t) * a + t * b;
 }
 
 /* common.jl:43-67 for the rank at (cx, cy) of a dimx x dimy grid: limits and counts */

@@ -203,11 +203,14 @@ static MarkerLayout marker_layout(int64_t md, double lx, double ly, double dx, d
     return marker_layout_rank(md, lx, ly, dx, dy, nx, ny, 0, 0, 1, 1);   // one rank: every side is physical
 }
 
-// Julia LinRange(a, b, n)[k] (1-based k): lerpi(k-1, n-1, a, b) = fma(t, b, fma(-t, a, a))
+// Julia LinRange(a, b, n)[k] (1-based k): lerpi(k-1, n-1, a, b) = (1 - t)*a + t*b with t = (k-1)/(n-1), two
+// products and a sum each rounded (this file is built without contraction).  That is the form the reference's
+// golden values fit: the fma form of lerpi moves some markers by one ulp, enough to put a marker of
+// test/test_StokesFlow2D.jl's case on the other side of the plume boundary
 __host__ __device__ __forceinline__ double linrange_at(double a, double b, int64_t n, int64_t k) {
     if (n == 1) return a;
     double t = (double)(k - 1) / (double)(n - 1);
-    return fma(t, b, fma(-t, a, a));
+    return (1.0 - t) * a + t * b;
 }
 
 __host__ __device__ __forceinline__ void marker_position(const MarkerLayout& L, double jitter, uint64_t seed,
