@@ -383,3 +383,87 @@ def exchange_markers(markers: dict, dims, lx, ly, dx, dy) -> dict:
                 parts.append(sent[(src, i)])
         out[(cx, cy)] = tuple(np.concatenate([p[q] for p in parts]) for q in range(4))
     return out
+
+
+# --------------------------------------------------------------------------
+# the StokesFlow2D timestep on a grid of ranks, composed from the pieces above
+# --------------------------------------------------------------------------
+# entries of each array beyond the rank's Nx x Ny grid (StokesFlow2D_multixpu.jl:89-109)
+_RANK_ARRAY_EXTRA = {"rho_vy": (1, 0), "mu_b": (0, 0), "mu_p": (-1, -1), "Vx": (2, 1), "Vy": (1, 2)}
+
+
+def rank_slices(name, coord, Nx, Ny):
+    """The global index range of a rank's array: ImplicitGlobalGrid with overlap 2 puts local point i of the
+    rank at coordinate c at global point c (N - 2) + i, in every array."""
+    sx, sy = _RANK_ARRAY_EXTRA[name]
+    x0, y0 = coord[0] * (Nx - 2), coord[1] * (Ny - 2)
+    return slice(x0, x0 + Nx + sx), slice(y0, y0 + Ny + sy)
+
+
+def rank_markers(dims, Nx, Ny, Lx, Ly, model: PlumeModel, marker_density, jitter=0.0, seed=0):
+    """initializeMarkersCPU + setInitialMarkerProperties! on every rank (StokesFlow2D_multixpu.jl:135-136):
+    {(cx, cy): (x, y, rho, mu)} in local coordinates; jitter with an odd density is followed by the exchange
+    (common.jl:93-97) before the properties are set; the jitter seed of a rank is seed + its MPI rank."""
+    nx_g, ny_g = dims[0] * (Nx - 2) + 2, dims[1] * (Ny - 2) + 2
+    dx, dy = Lx / (nx_g - 1), Ly / (ny_g - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    out = {}
+    for cx in range(dims[0]):
+        for cy in range(dims[1]):
+            x, y = initialize_markers_rank(marker_density, lx, ly, dx, dy, Nx, Ny, (cx, cy), dims, jitter,
+                                           seed + cx * dims[1] + cy)
+            out[(cx, cy)] = (x, y, np.zeros_like(x), np.zeros_like(x))
+    if jitter != 0.0 and marker_density % 2 == 1:
+        out = exchange_markers(out, dims, lx, ly, dx, dy)
+    for (cx, cy), (x, y, _, _) in out.items():
+        rho, mu = set_marker_properties(model, x, y, cx * (Nx - 2) * dx, cy * (Ny - 2) * dy)
+        out[(cx, cy)] = (x, y, rho, mu)
+    return out
+
+
+def stokes_flow_2d_ranks(Nt, dims, Nx, Ny, Lx, Ly, markers: dict, stokes_eps=1e-5, iter_max=100000, g_y=9.81,
+                         maxdisp=0.5, nthreads=1):
+    """StokesFlow2D_multixpu.jl:157-191 on dims[0] x dims[1] ranks of Nx x Ny local points, from oracle pieces:
+    per-rank deposits onto the (Nx+1, Ny) interpolation arrays, sumOverlappingValues!, safeDivision; the solve
+    on the global grid (the decomposed PT iterate is the global one; the stopping test uses the one-rank err,
+    which only moves the stopping iteration); per-rank RK4 on the local slices of V; exchangeMarkers.
+    markers: {(cx, cy): (x, y, rho, mu)} in local coordinates (rank_markers).  Returns (Vx_glob, Vy_glob,
+    t_tot, markers, dts) with V as gather_V_grid hands it back."""
+    nx_g, ny_g = dims[0] * (Nx - 2) + 2, dims[1] * (Ny - 2) + 2
+    dx, dy = Lx / (nx_g - 1), Ly / (ny_g - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    o = node_origins(dx, dy)
+    a = stokes_arrays(nx_g, ny_g)
+    grids = {c: {n: zeros(Nx + s[0], Ny + s[1]) for n, s in _RANK_ARRAY_EXTRA.items() if n not in ("Vx", "Vy")}
+             for c in markers}
+    markers = {c: tuple(v.copy() for v in m) for c, m in markers.items()}
+    dt, t_tot, dts = 0.0, 0.0, []
+    for _ in range(Nt):
+        for name, (xo, yo), q in (("rho_vy", ("x_rho", "y_rho"), 2), ("mu_b", ("x", "y"), 3),
+                                  ("mu_p", ("x_p", "y_p"), 3)):                    # :164-166
+            vws = {c: zeros(Nx + 1, Ny) for c in markers}
+            ws = {c: zeros(Nx + 1, Ny) for c in markers}
+            for c, m in markers.items():
+                bilinear_marker_to_grid(o[xo], o[yo], grids[c][name], m[0], m[1], m[q], dx, dy, vws[c], ws[c])
+            sum_overlapping_values(ws, dims, Nx, Ny)
+            sum_overlapping_values(vws, dims, Nx, Ny)
+            for c in markers:                                                     # safeDivision
+                g = grids[c][name]
+                nxv, nyv = g.shape
+                nz = ws[c][:nxv, :nyv] != 0
+                g[nz] = vws[c][:nxv, :nyv][nz] / ws[c][:nxv, :nyv][nz]
+                xs, ys = rank_slices(name, c, Nx, Ny)
+                a[name][xs, ys] = g
+        r = solve_stokes(a, g_y, dx, dy, nx_g, ny_g, dt, maxdisp, True, stokes_eps, iter_max, nthreads)
+        dt = r.dt
+        dts.append(dt)
+        for c, m in markers.items():                                              # :181, local domain
+            xs, ys = rank_slices("Vx", c, Nx, Ny)
+            vx = np.asfortranarray(a["Vx"][xs, ys])
+            xs, ys = rank_slices("Vy", c, Nx, Ny)
+            vy = np.asfortranarray(a["Vy"][xs, ys])
+            move_markers_rk4(m[0], m[1], vx, vy, o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy,
+                             nthreads)
+        markers = exchange_markers(markers, dims, lx, ly, dx, dy)                # :186-191
+        t_tot += dt
+    return a["Vx"], a["Vy"], t_tot, markers, dts

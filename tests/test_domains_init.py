@@ -117,3 +117,23 @@ def test_decomposed_flow_from_model_steps(sf):
     rec = flow.step()
     assert rec["dt"] > 0 and rec["info"]["converged"]
     assert all(torch.isfinite(v).all() for v in flow.velocities())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,nx,ny", [((2, 2), 11, 14), ((3, 2), 8, 14), ((1, 3), 20, 10)])
+def test_decomposed_flow_meets_the_reference_golden_values(sf, dims, nx, ny):
+    """test/test_StokesFlow2D.jl:91-110 on the GPU's decomposed timestep: the 20 x 26-point plume case split
+    over the reference's rank grids, 5 timesteps, markers laid out by the ranks, the reference's golden values
+    at its tolerance (atol 1e-6)."""
+    from fields import golden
+    g = golden()["stokes_flow_2d"]
+    model = sf.PlumeModel(**g["model"])
+    flow = domains.DecomposedStokesFlow2D(dims, nx, ny, g["Lx"], g["Ly"], model=model,
+                                          marker_density=g["marker_density"], eps=g["stokes_eps"])
+    for _ in range(g["Nt"]):
+        flow.step()
+    vx, vy = (v.cpu().numpy() for v in flow.velocities())
+    assert vx.shape == (g["Nx"] + 2, g["Ny"] + 1) and vy.shape == (g["Nx"] + 1, g["Ny"] + 2)
+    inds = np.array(g["inds"]) - 1
+    assert np.allclose(vx.ravel(order="F")[inds], g["vx_ref"], rtol=0, atol=g["atol"])
+    assert np.allclose(vy.ravel(order="F")[inds], g["vy_ref"], rtol=0, atol=g["atol"])

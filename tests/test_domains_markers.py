@@ -129,43 +129,10 @@ def _initial_markers(dims, Nx, Ny, dx, dy, per_rank, seed):
 
 
 def _oracle_decomposed_steps(mk, dims, Nx, Ny, Lx, Ly, steps, iters):
-    """The decomposed timestep from oracle pieces: per-rank deposits + overlap sums + safeDivision, the solve
-    on the global grid (the decomposed iterate equals it), per-rank RK4 on the local slices, the exchange."""
-    nx_g, ny_g = domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)
-    dx, dy = Lx / (nx_g - 1), Ly / (ny_g - 1)
-    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
-    o = oracle.node_origins(dx, dy)
-    a = oracle.stokes_arrays(nx_g, ny_g)
-    ranks = {c: {n: oracle.zeros(Nx + s[0], Ny + s[1]) for n, s in (("rho_vy", (1, 0)), ("mu_b", (0, 0)), ("mu_p", (-1, -1)))}
-             for c in mk}
-    markers = {c: tuple(v.copy() for v in m) for c, m in mk.items()}
-    dt, dts = 0.0, []
-    for _ in range(steps):
-        for name, (xo, yo), q in (("rho_vy", ("x_rho", "y_rho"), 2), ("mu_b", ("x", "y"), 3), ("mu_p", ("x_p", "y_p"), 3)):
-            vws = {c: oracle.zeros(Nx + 1, Ny) for c in mk}
-            ws = {c: oracle.zeros(Nx + 1, Ny) for c in mk}
-            for c, m in markers.items():
-                oracle.bilinear_marker_to_grid(o[xo], o[yo], ranks[c][name], m[0], m[1], m[q], dx, dy, vws[c], ws[c])
-            oracle.sum_overlapping_values(ws, dims, Nx, Ny)
-            oracle.sum_overlapping_values(vws, dims, Nx, Ny)
-            for c in mk:
-                g = ranks[c][name]
-                nxv, nyv = g.shape
-                nz = ws[c][:nxv, :nyv] != 0
-                g[nz] = vws[c][:nxv, :nyv][nz] / ws[c][:nxv, :nyv][nz]
-                xs, ys = domains.local_slices(name, c, Nx, Ny)
-                a[name][xs, ys] = g
-        r = oracle.solve_stokes(a, 9.81, dx, dy, nx_g, ny_g, dt, 0.5, True, 1e-300, iters, 4)
-        dt = r.dt
-        dts.append(dt)
-        for c, m in markers.items():
-            xs, ys = domains.local_slices("Vx_pad", c, Nx, Ny)
-            vx = np.asfortranarray(a["Vx"][xs, ys])
-            xs, ys = domains.local_slices("Vy_pad", c, Nx, Ny)
-            vy = np.asfortranarray(a["Vy"][xs, ys])
-            oracle.move_markers_rk4(m[0], m[1], vx, vy, o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy, 1)
-        markers = oracle.exchange_markers(markers, dims, lx, ly, dx, dy)
-    return markers, a, dts
+    """The decomposed timestep from oracle pieces (oracle.stokes_flow_2d_ranks), a fixed iteration count."""
+    vx, vy, _, markers, dts = oracle.stokes_flow_2d_ranks(steps, dims, Nx, Ny, Lx, Ly, mk, stokes_eps=1e-300,
+                                                          iter_max=iters, nthreads=4)
+    return markers, {"Vx": vx, "Vy": vy}, dts
 
 
 @pytest.mark.gpu

@@ -227,3 +227,27 @@ def test_linrange_form_decides_a_boundary_marker(oracle_lib):
     assert x[k] == 5.0 and y[k] == 3.0
     rho, _ = O.set_marker_properties(O.PlumeModel(**g["model"]), x[k:k + 1], y[k:k + 1])
     assert rho[0] == g["model"]["rho_matrix"]
+
+
+# test/test_StokesFlow2D.jl:16-51: the same 20 x 26-point global grid split over 1 to 9 ranks
+RANK_GRIDS = [((1, 1), 20, 26), ((1, 2), 20, 14), ((2, 1), 11, 26), ((1, 3), 20, 10), ((3, 1), 8, 26),
+              ((2, 2), 11, 14), ((2, 3), 11, 10), ((3, 2), 8, 14), ((3, 3), 8, 10)]
+
+
+@pytest.mark.parametrize("dims,nx,ny", RANK_GRIDS)
+def test_stokes_flow_2d_golden_on_ranks(oracle_lib, dims, nx, ny):
+    """test/test_StokesFlow2D.jl:91-110 on every rank grid the reference runs it on: the rank layouts of
+    initializeMarkersCPU, the overlap sums of the deposits, the marker exchange and gather_V_grid, composed from
+    the oracle's pieces, give the reference's golden values at its tolerance (atol 1e-6) in every split."""
+    O = oracle_lib
+    g = golden()["stokes_flow_2d"]
+    model = O.PlumeModel(**g["model"])
+    mk = O.rank_markers(dims, nx, ny, g["Lx"], g["Ly"], model, g["marker_density"])
+    assert sum(v[0].size for v in mk.values()) == (g["marker_density"] * (g["Nx"] - 1)) * \
+        (g["marker_density"] * (g["Ny"] - 1))                                    # the ranks tile the lattice
+    Vx, Vy, t_tot, _, _ = O.stokes_flow_2d_ranks(g["Nt"], dims, nx, ny, g["Lx"], g["Ly"], mk,
+                                                 stokes_eps=g["stokes_eps"])
+    assert Vx.shape == (g["Nx"] + 2, g["Ny"] + 1) and Vy.shape == (g["Nx"] + 1, g["Ny"] + 2)   # :103-104
+    inds = np.array(g["inds"]) - 1
+    assert np.allclose(Vx.ravel(order="F")[inds], g["vx_ref"], rtol=0, atol=g["atol"])      # :107
+    assert np.allclose(Vy.ravel(order="F")[inds], g["vy_ref"], rtol=0, atol=g["atol"])      # :108
