@@ -137,3 +137,44 @@ def test_decomposed_flow_meets_the_reference_golden_values(sf, dims, nx, ny):
     inds = np.array(g["inds"]) - 1
     assert np.allclose(vx.ravel(order="F")[inds], g["vx_ref"], rtol=0, atol=g["atol"])
     assert np.allclose(vy.ravel(order="F")[inds], g["vy_ref"], rtol=0, atol=g["atol"])
+
+
+# test/test_InitialMarkerCoords.jl:17-56: the 20 x 26-point global grid on 1 to 9 ranks
+INIT_GRIDS = [((1, 1), 20, 26), ((1, 2), 20, 14), ((2, 1), 11, 26), ((1, 3), 20, 10), ((3, 1), 8, 26),
+              ((1, 4), 20, 8), ((2, 3), 11, 10), ((3, 2), 8, 14), ((2, 4), 11, 8), ((3, 3), 8, 10)]
+
+
+@pytest.mark.parametrize("dims,nx,ny", INIT_GRIDS)
+def test_reference_initial_marker_coords_on_ranks(dims, nx, ny):
+    """test/test_InitialMarkerCoords.jl:67-134 as the reference runs it: 3 markers per cell, the ranks' layouts
+    gathered with gather_markers! and sorted by x * Lx * 2 + y equal the global lattice (same count; `≈` on the
+    whole vectors)."""
+    md, Lx, Ly = 3, 10.0, 10.0
+    nxg, nyg = domains.global_size(dims[0], nx), domains.global_size(dims[1], ny)
+    assert (nxg, nyg) == (20, 26)
+    dx, dy = Lx / (nxg - 1), Ly / (nyg - 1)
+    lx, ly = (nx - 1) * dx, (ny - 1) * dy
+    ranks = {}
+    for c in coords_of(dims):
+        x, y = oracle.initialize_markers_rank(md, lx, ly, dx, dy, nx, ny, c, dims)
+        z = torch.zeros(x.size, dtype=torch.float64)
+        ranks[c] = (torch.from_numpy(x), torch.from_numpy(y), z, z)
+    xg, yg, _, _ = (t.numpy() for t in domains.gather_markers(ranks, dims, lx, ly, dx, dy))
+    order = np.argsort(xg * Lx * 2 + yg, kind="stable")
+    xg, yg = xg[order], yg[order]
+    # the reference lattice (:101-124), LinRange elements as (1 - t) a + t b
+    nmx, nmy = md * (nxg - 1), md * (nyg - 1)
+    dxm, dym = dx / md, dy / md
+
+    def linrange(a, b, n):
+        t = np.arange(n) / (n - 1)
+        return (1 - t) * a + t * b
+
+    xr = np.repeat(linrange(0.5 * dxm, Lx - 0.5 * dxm, nmx), nmy)
+    yr = np.tile(linrange(0.5 * dym, Ly - 0.5 * dym, nmy), nmx)
+    order = np.argsort(xr * Lx * 2 + yr, kind="stable")
+    xr, yr = xr[order], yr[order]
+    assert xg.size == xr.size == nmx * nmy                                            # :126-127
+    tol = np.sqrt(np.finfo(np.float64).eps)                                           # isapprox's default rtol
+    assert np.linalg.norm(xg - xr) <= tol * max(np.linalg.norm(xg), np.linalg.norm(xr))   # :129
+    assert np.linalg.norm(yg - yr) <= tol * max(np.linalg.norm(yg), np.linalg.norm(yr))   # :130
