@@ -107,3 +107,40 @@ def test_decomposed_solve_is_the_global_solve(sf, dims):
             assert torch.equal(loc[name], g[name][xs, ys]), f"rank {coord} {name}"
     for name in ("Vx_pad", "Vy_pad", "P"):   # what gather_V_grid hands back
         assert torch.equal(domains.gather(ranks, name, dims, Nx, Ny), g[name]), name
+
+
+# test/test_StokesSolver.jl:17-41: the 26 x 32-point global grid on 1 to 4 ranks
+SOLVER_GRIDS = [((1, 2), 26, 17), ((2, 1), 14, 32), ((1, 3), 26, 12), ((3, 1), 10, 32), ((4, 1), 8, 32),
+                ((2, 2), 14, 17)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dims,Nx,Ny", SOLVER_GRIDS)
+def test_decomposed_solve_meets_the_solver_golden_values(sf, dims, Nx, Ny):
+    """test/test_StokesSolver.jl:48-140 on the reference's rank grids, through the decomposed solve (halo updates,
+    the multi-rank err and dt): the gathered velocities match the reference's golden values as its `≈` does
+    (norm-relative sqrt(eps)), and the free-slip / mirror identities of the padded arrays hold exactly."""
+    from fields import golden, solver_test_fields
+    g = golden()["stokes_solver"]
+    nx_g, ny_g, dx, dy = g["Nx"], g["Ny"], g["dx"], g["dy"]
+    assert (domains.global_size(dims[0], Nx), domains.global_size(dims[1], Ny)) == (nx_g, ny_g)
+    rho, mub, mup = solver_test_fields(nx_g, ny_g, dx, dy)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a).T)).cuda().t()  # noqa: E731
+    z = sf.zeros
+    glob = {"rho_vy": dev(rho), "mu_b": dev(mub), "mu_p": dev(mup), "P": z(nx_g - 1, ny_g - 1),
+            "Vx_s": z(nx_g, ny_g + 1), "Vy_s": z(nx_g + 1, ny_g), "dVxdt": z(nx_g - 2, ny_g - 1),
+            "dVydt": z(nx_g - 1, ny_g - 2), "Vx_pad": z(nx_g + 2, ny_g + 1), "Vy_pad": z(nx_g + 1, ny_g + 2)}
+    ranks = domains.split(glob, dims, Nx, Ny)
+    info = domains.solve_stokes_decomposed(ranks, dims, Nx, Ny, g["g_y"], dx, dy, 0.0, g["maxdisp"], eps=g["eps"],
+                                           iter_max=100000)
+    assert info["converged"] == 1
+    vx = domains.gather(ranks, "Vx_pad", dims, Nx, Ny).cpu().numpy()
+    vy = domains.gather(ranks, "Vy_pad", dims, Nx, Ny).cpu().numpy()
+    inds = np.array(g["inds"]) - 1
+    tol = np.sqrt(np.finfo(np.float64).eps)
+    for got, ref in ((vx.ravel(order="F")[inds], np.array(g["vx_ref"])), (vy.ravel(order="F")[inds], np.array(g["vy_ref"]))):
+        assert np.linalg.norm(got - ref) <= tol * max(np.linalg.norm(got), np.linalg.norm(ref))
+    assert np.array_equal(vx[0], -vx[2]) and np.all(vx[1] == 0) and np.array_equal(vx[-1], -vx[-3]) and np.all(vx[-2] == 0)
+    assert np.array_equal(vx[:, 0], vx[:, 1]) and np.array_equal(vx[:, -1], vx[:, -2])
+    assert np.array_equal(vy[:, 0], -vy[:, 2]) and np.all(vy[:, 1] == 0) and np.array_equal(vy[:, -1], -vy[:, -3])
+    assert np.all(vy[:, -2] == 0) and np.array_equal(vy[0], vy[1]) and np.array_equal(vy[-1], vy[-2])
