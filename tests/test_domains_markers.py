@@ -154,3 +154,53 @@ def test_decomposed_timesteps_match_oracle(sf, dims):
             assert np.array_equal(st.markers[c][q].cpu().numpy(), ref_markers[c][q]), (c, q)
     moved = sum(abs(len(ref_markers[c][0]) - len(mk[c][0])) for c in mk)
     assert moved > 0          # markers did cross between ranks
+
+
+def test_reference_marker_to_grid_multi_process():
+    """test/test_MarkerToGrid.jl:43-148 (TEST 2) as the reference runs it: 2 x 2 ranks of 10 x 8 points, 25
+    random markers per cell in each rank's own part of the domain, deposited per rank onto three grids (origins
+    (dx/2, dy/2), (0, 0), (-dx/2, 0)) with sumOverlappingValues! on the (Nx+1, Ny) sums and safeDivision,
+    gathered as create_grid_view does; a one-process deposit of the gathered markers onto the global grids
+    agrees elementwise at isapprox's default tolerance."""
+    dims, Nx, Ny, dx, dy = (2, 2), 10, 8, 0.3, 0.4
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    origins = {"mu_p": (0.5 * dx, 0.5 * dy), "mu_b": (0.0, 0.0), "rho_vy": (-0.5 * dx, 0.0)}   # grid1..3, :62-67
+    rng = np.random.default_rng(2)
+    nm = 25 * (Nx - 1) * (Ny - 1)
+    markers = {}
+    for cx in range(2):
+        for cy in range(2):
+            rank = cx * 2 + cy
+            x = rng.random(nm) * (lx - 0.5 * dx) + (0.5 * dx if cx > 0 else 0.0)      # :75-77
+            y = rng.random(nm) * (ly - 0.5 * dy) + (0.5 * dy if cy > 0 else 0.0)
+            markers[(cx, cy)] = (x, y, rng.random(nm) + 2 * (rank + 1))
+    local = {}
+    for name, (gx, gy) in origins.items():
+        sx, sy = domains.ARRAYS[name]
+        grids = {c: oracle.zeros(Nx + sx, Ny + sy) for c in markers}
+        vws = {c: oracle.zeros(Nx + 1, Ny) for c in markers}
+        ws = {c: oracle.zeros(Nx + 1, Ny) for c in markers}
+        for c, (x, y, v) in markers.items():
+            oracle.bilinear_marker_to_grid(gx, gy, grids[c], x, y, v, dx, dy, vws[c], ws[c])
+        oracle.sum_overlapping_values(ws, dims, Nx, Ny)
+        oracle.sum_overlapping_values(vws, dims, Nx, Ny)
+        for c in markers:
+            g = grids[c]
+            nz = ws[c][:g.shape[0], :g.shape[1]] != 0
+            g[nz] = vws[c][:g.shape[0], :g.shape[1]][nz] / ws[c][:g.shape[0], :g.shape[1]][nz]
+        local[name] = {c: {name: torch.from_numpy(np.ascontiguousarray(g))} for c, g in grids.items()}
+    # gather_markers! (:88) and the one-process deposit (:119-138)
+    xg, yg, vg, _ = (t.numpy() for t in domains.gather_markers(
+        {c: tuple(torch.from_numpy(a) for a in (x, y, v, v)) for c, (x, y, v) in markers.items()}, dims, lx, ly, dx,
+        dy))
+    nxg, nyg = domains.global_size(2, Nx), domains.global_size(2, Ny)
+    assert (nxg, nyg) == (18, 14)
+    tol = np.sqrt(np.finfo(np.float64).eps)
+    for name, (gx, gy) in origins.items():
+        sx, sy = domains.ARRAYS[name]
+        single = oracle.zeros(nxg + sx, nyg + sy)
+        vws, ws = oracle.zeros(nxg + 1, nyg), oracle.zeros(nxg + 1, nyg)
+        oracle.bilinear_marker_to_grid(gx, gy, single, xg, yg, vg, dx, dy, vws, ws)
+        multi = domains.gather(local[name], name, dims, Nx, Ny).numpy()
+        assert multi.shape == single.shape
+        assert np.all(np.abs(multi - single) <= tol * np.maximum(np.abs(multi), np.abs(single))), name   # :141-143
