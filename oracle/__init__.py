@@ -14,6 +14,16 @@ reference's floating-point expression order:
 * ``scripts/StokesSolver_multixpu.jl``   solveStokes! (pseudo-transient iteration)
 * ``scripts/MoveMarkers.jl:15-187``      moveMarkersRK4!, interpolateV
 
+plus numpy restatements of the pieces that cross ranks (``sumOverlappingValues!``,
+``exchangeMarkers``) and a composition of the decomposed timestep from them.
+
+Pinned against every known-answer test the reference holds for this path, at
+the reference's own tolerances: test_StokesSolver.jl, test_MarkerToGrid.jl,
+test_MoveMarkers.jl, test_InitialMarkerCoords.jl, the three
+test_MarkerExchange_*.jl and test_StokesFlow2D.jl, the last four also on the
+rank grids the reference runs them on (tests/test_oracle_golden.py,
+tests/test_oracle_exchange_reference.py, tests/test_domains*.py).
+
 Grid arrays are numpy arrays in Fortran order with the Julia shape, so
 ``A[ix-1, iy-1]`` is Julia's ``A[ix, iy]`` and ``A.ravel(order="F")`` is
 Julia's linear indexing.
