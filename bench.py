@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--iter-max", type=int, default=400000,
                     help="PT iteration cap per solve (reference default 100000; a cold 2048^2 start needs ~250k)")
     ap.add_argument("--mu-air", type=float, default=1e-2,
-                    help="air viscosity; 1e-3 makes the reference PT scheme diverge (see DESIGN.md)")
+                    help="air viscosity; with 1e-3 (a 1000x jump) the reference PT scheme diverges")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=12, help="PT iterations in the CPU baseline sample")

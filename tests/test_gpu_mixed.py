@@ -2,7 +2,7 @@
 
 * accuracy: FP64 defect correction around FP32 sweeps reaches the same
   discrete solution as the plain FP64 solver; relative L2 difference of V and
-  P stated at the stopping tolerance (1e-5 at relative
+  P stated at the stopping tolerance (required bar: 1e-5 at relative
   residual 1e-6);
 * batch invariance: an instance solved inside a batch of differently sized
   instances gives bit-identical results to the same instance solved alone

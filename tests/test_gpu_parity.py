@@ -5,7 +5,7 @@ oracle (same expression order, no FMA contraction, reference summation order
 in the deposit).  The only floating-point difference allowed anywhere is the
 summation order inside the residual norm `err`, which can only move the
 stopping iteration when err lands within ~1e-15 of eps; the full-timestep
-tests therefore also check the north-star bar (1e-10 relative L2) explicitly.
+tests therefore also check the required bar (1e-10 relative L2) explicitly.
 """
 import math
 
