@@ -397,7 +397,8 @@ typedef struct {
 int sf_engine_instance_bytes(int64_t Nx, int64_t Ny, int64_t* bytes);
 
 /* opt may be NULL (the defaults of sf_mixed_options).  The arena is
- * allocated here, once. */
+ * allocated here, once.  The engine uses ctx (its device, its record of the
+ * tuner's choices) for its whole life: destroy the engine first. */
 int sf_engine_create(sf_ctx* ctx, int64_t arena_bytes, int32_t max_instances, const sf_mixed_options* opt,
                      sf_engine** out);
 /* Waits for the engine's work, then frees it.  Instances still admitted are
