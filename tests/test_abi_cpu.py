@@ -137,3 +137,17 @@ def test_api_rejects_host_tensors():
 def test_node_origins_match_reference_formulas(oracle_lib):
     dx, dy = 10 / 19, 10 / 25
     assert sf.node_origins(dx, dy) == oracle_lib.node_origins(dx, dy)
+
+
+def test_engine_instance_bytes_is_the_arena_layout(L):
+    """An instance's arena block: 14 FP32 fields then 6 FP64 fields, each field LD x (Ny + 3) entries with
+    LD = roundup(Nx + 4, 32), each part rounded up to 256 B.  Serving admits requests by this figure."""
+    b = C.c_int64()
+    for nx, ny in ((4, 4), (64, 64), (127, 1023), (2048, 2048), (1000, 33)):
+        assert L.sf_engine_instance_bytes(nx, ny, C.byref(b)) == 0
+        ld = -(-(nx + 4) // 32) * 32
+        f = ld * (ny + 3)
+        r256 = lambda v: -(-v // 256) * 256  # noqa: E731
+        assert b.value == r256(14 * f * 4) + r256(6 * f * 8), (nx, ny)
+    assert L.sf_engine_instance_bytes(3, 10, C.byref(b)) == _lib.SF_ERR_INVALID_ARG
+    assert sf.Engine.instance_bytes(64, 64) == r256(14 * 96 * 67 * 4) + r256(6 * 96 * 67 * 8)
