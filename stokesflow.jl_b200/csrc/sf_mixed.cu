@@ -800,15 +800,16 @@ struct sf_engine {
     int graph_k[NCAND] = {};
     int blocks = 0;                      // persistent CTAs of the current shape
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-    // sweep shape and its autotuner: while measuring, each round's sweeps run in the next shape to try and are
-    // timed on the engine stream; the shape with the fewest ns per point-sweep is kept and recorded in the context
+    // the sweep candidate in use (shape, schedule, launch mode) and its tuner: the first round of a workload
+    // class the context has not seen starts with short timed pieces of every candidate on the engine stream; the
+    // candidate with the fewest ns per point-sweep is then used and recorded in the context for that class
     int shape = DEFAULT_SHAPE;
     int sched = 0;
     int overlap = 0;
     int tune_state = SF_TUNE_MEASURING;
-    int tune_trials = 0;
-    int tune_key = -1;
-    double tune_ns[NCAND] = {};          // best ns per point-sweep of each candidate (0: not measured)
+    int tune_trials = 0;                 // pieces timed so far for the class being measured
+    int tune_key = -1;                   // workload class of the current sweep set
+    double tune_ns[NCAND] = {};          // the last completed measurement, ns per point-sweep (0: not measured)
     int timed_first = 0;                 // the last round timed trials timed_first ...
     int timed_pieces = 0;                // ... up to timed_first + timed_pieces - 1 (candidate = trial % NCAND),
     double timed_points = 0.0;           // each piece over this many point-sweeps
