@@ -492,7 +492,8 @@ def run_precision_form(a):
                           "fp64_iters": int(rec["fp64"]["info"]["iters"]),
                           "mixed_sweeps": int(rec["mixed"]["info"]["inner_iters"]),
                           "rel_l2_Vx": _rel_l2(m.Vx, f.Vx), "rel_l2_Vy": _rel_l2(m.Vy, f.Vy),
-                          "rel_l2_P": _rel_l2(m.P, f.P), "rel_l2_markers_x": _rel_l2(m.x_m, f.x_m)})
+                          "rel_l2_P": _rel_l2(m.P, f.P), "rel_l2_markers_x": _rel_l2(m.x_m, f.x_m),
+                          "rel_l2_markers_y": _rel_l2(m.y_m, f.y_m)})
         fs = sum(s["fp64_solve_ms"] for s in steps)
         ms = sum(s["mixed_solve_ms"] for s in steps)
         cases.append({"contrast": contrast, "mu_plume": model.mu_plume, "fp64_solve_ms_total": round(fs, 1),
@@ -500,7 +501,8 @@ def run_precision_form(a):
         del states
         torch.cuda.empty_cache()
     clk = clocks.stop()
-    worst = {k: max(s[k] for cs in cases for s in cs["steps"]) for k in ("rel_l2_Vx", "rel_l2_Vy", "rel_l2_P")}
+    worst = {k: max(s[k] for cs in cases for s in cs["steps"]) for k in ("rel_l2_Vx", "rel_l2_Vy", "rel_l2_P",
+                                                                       "rel_l2_markers_x", "rel_l2_markers_y")}
     fs = sum(cs["fp64_solve_ms_total"] for cs in cases)
     ms = sum(cs["mixed_solve_ms_total"] for cs in cases)
     return {"form": "precision", "metric": f"solve time and rel L2 vs plain FP64, relative residual {a.rtol:g}",
