@@ -127,7 +127,8 @@ typedef struct {
     int32_t converged;       /* err <= eps                                                             */
     int32_t reserved;
     double loop_ms;          /* device time of the whole iteration loop                                */
-    double bytes_per_iter;   /* essential HBM bytes of one fused PT iteration (see DESIGN)             */
+    double bytes_per_iter;   /* essential HBM bytes of one fused PT iteration: 8*[2*(|Vx_s|+|Vy_s|+|P|+  */
+                             /* |dVx|+|dVy|) + |rho_vy|+|mu_b|+|mu_p|], about 104*Nx*Ny                */
     double T_eff_essential;  /* bytes_per_iter * iters / loop time, GB/s                               */
     int64_t fused_launches;  /* launches of the fused PT iteration kernel                              */
     double fused_ms;         /* device time of the fused launches alone (0 unless timing requested)    */
