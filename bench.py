@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=2048, help="grid points per side (cells = n - 1)")
+    ap.add_argument("--n", "--grid-points", dest="n", type=int, default=2048,
+                    help="grid points per side (cells = n - 1); under torchrun spell it --grid-points, since "
+                         "torchrun's own parser takes --n for a prefix of its options")
     ap.add_argument("--markers-per-cell", type=int, default=16)
     ap.add_argument("--rtol", type=float, default=1e-6)
     ap.add_argument("--iter-max", type=int, default=400000,
