@@ -151,3 +151,50 @@ def test_engine_instance_bytes_is_the_arena_layout(L):
         assert b.value == r256(14 * f * 4) + r256(6 * f * 8), (nx, ny)
     assert L.sf_engine_instance_bytes(3, 10, C.byref(b)) == _lib.SF_ERR_INVALID_ARG
     assert sf.Engine.instance_bytes(64, 64) == r256(14 * 96 * 67 * 4) + r256(6 * 96 * 67 * 8)
+
+
+def _ctypes_for_c(decl):
+    """The ctypes types a C parameter (or return type) declaration may be bound with, by kind and width."""
+    t = re.sub(r"\s+", "", re.sub(r"\b[A-Za-z_]\w*$", "", decl.strip()) if re.search(r"[\s*]\w+$", decl.strip())
+               else decl)
+    t = t.replace("const", "")
+    structs = {c.__doc__.strip().rstrip("."): c for c in vars(_lib).values()
+               if isinstance(c, type) and issubclass(c, C.Structure) and c.__doc__}
+    scalars = {"double": (C.c_double,), "int64_t": (C.c_int64,), "int": (C.c_int, C.c_int32),
+               "int32_t": (C.c_int32, C.c_int), "uint64_t": (C.c_uint64,), "char*": (C.c_char_p,)}
+    if t in scalars:
+        return scalars[t]
+    if t in ("void*", "sf_ctx*", "sf_engine*"):
+        return (C.c_void_p,)
+    if t in ("sf_ctx**", "sf_engine**"):
+        return (C.POINTER(C.c_void_p),)
+    if t == "double*":                   # a device array passed as an address, or a host result
+        return (C.c_void_p, C.POINTER(C.c_double))
+    if t in ("int64_t*", "int32_t*"):   # a host result, or a device array passed as an address
+        return (C.POINTER(scalars[t[:-1]][0]), C.c_void_p)
+    if t.endswith("*") and t[:-1] in structs:
+        return (C.POINTER(structs[t[:-1]]),)
+    raise AssertionError(f"no ctypes rule for {decl!r}")
+
+
+def _header_prototypes():
+    text = re.sub(r"/\*.*?\*/", " ", "".join(open(h).read() for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h")))), flags=re.S)
+    out = {}
+    for m in re.finditer(r"\n\s*((?:const\s+)?[A-Za-z_]\w*\s*\**)\s*(sf_\w+)\s*\(([^;]*?)\)\s*;", text):
+        params = m.group(3).strip()
+        out[m.group(2)] = (m.group(1), [] if params in ("", "void") else [p.strip() for p in params.split(",")])
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(_lib.PROTOTYPES))
+def test_ctypes_prototype_matches_header(name):
+    """Each ctypes prototype passes one argument per C parameter, of the same kind and width, so that no
+    call truncates an int64_t or shifts the arguments after it."""
+    protos = _header_prototypes()
+    assert name in protos
+    cret, cparams = protos[name]
+    res, args = _lib.PROTOTYPES[name]
+    assert res in _ctypes_for_c(cret), f"{name}: returns {cret}, bound as {res}"
+    assert len(args) == len(cparams), f"{name}: {len(args)} ctypes arguments for {len(cparams)} C parameters"
+    for k, (a, p) in enumerate(zip(args, cparams)):
+        assert a in _ctypes_for_c(p), f"{name}: parameter {k} ({p}) bound as {a}"
