@@ -251,3 +251,27 @@ def test_stokes_flow_2d_golden_on_ranks(oracle_lib, dims, nx, ny):
     inds = np.array(g["inds"]) - 1
     assert np.allclose(Vx.ravel(order="F")[inds], g["vx_ref"], rtol=0, atol=g["atol"])      # :107
     assert np.allclose(Vy.ravel(order="F")[inds], g["vy_ref"], rtol=0, atol=g["atol"])      # :108
+
+
+def test_oracle_threads_do_not_change_bits(oracle_lib):
+    """The timed CPU baseline and the full-size GPU parity test run the oracle's stencil and advection on
+    several OpenMP threads: every array, dt, err and the iteration count are the same bits as on one thread
+    (each point is written by one thread, and the residual means are summed serially)."""
+    O = oracle_lib
+    g = golden()["stokes_solver"]
+    Nx, Ny, dx, dy = g["Nx"], g["Ny"], g["dx"], g["dy"]
+    runs = {}
+    for nt in (1, 4):
+        a = O.stokes_arrays(Nx, Ny)
+        a["rho_vy"][:], a["mu_b"][:], a["mu_p"][:] = solver_test_fields(Nx, Ny, dx, dy)
+        r = O.solve_stokes(a, g["g_y"], dx, dy, Nx, Ny, 0.0, g["maxdisp"], True, g["eps"], 100000, nthreads=nt)
+        o = O.node_origins(dx, dy)
+        x, y = O.initialize_markers(4, dx * (Nx - 1), dy * (Ny - 1), dx, dy, Nx, Ny, 0.5, 3)
+        nf = O.move_markers_rk4(x, y, a["Vx"], a["Vy"], o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], r.dt,
+                                dx * (Nx - 1), dy * (Ny - 1), dx, dy, nthreads=nt)
+        runs[nt] = (a, r, x, y, nf)
+    (a1, r1, x1, y1, f1), (a4, r4, x4, y4, f4) = runs[1], runs[4]
+    assert (r1.dt, r1.err, r1.iters, r1.n_checks) == (r4.dt, r4.err, r4.iters, r4.n_checks)
+    for k in a1:
+        assert np.array_equal(a1[k], a4[k]), k
+    assert np.array_equal(x1, x4) and np.array_equal(y1, y4) and f1 == f4
