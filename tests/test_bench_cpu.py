@@ -42,3 +42,12 @@ def test_reference_arm_under_torchrun_prints_once():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_own_arm_fails_loudly_without_a_gpu():
+    """No CPU fallback: without a CUDA device the benchmark's own arm exits non-zero and prints no line."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "bench.py", "--steps", "1", "--warmup", "3", "--n", "64", "--no-cpu-baseline"],
+                       cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0
+    assert not [ln for ln in r.stdout.splitlines() if ln.strip().startswith("{")]
