@@ -84,14 +84,23 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--batch-cells", default="127,1023", help="cells per side, log-uniform range")
     ap.add_argument("--mu-log10", default="-2,1", help="inclusion viscosity range (log10), log-uniform")
-    ap.add_argument("--fp64-sample", type=int, default=0,
-                    help="batch form: time the FP64 loop on the first K instances only (0: all)")
+    ap.add_argument("--fp64-concurrency", type=int, default=8,
+                    help="batch and serve forms: also time plain FP64 with this many solves at a time (host "
+                         "threads, own contexts and streams); 1: only one at a time")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--serve-requests", type=int, default=24)
-    ap.add_argument("--serve-rate", type=float, default=2.0, help="requests per second (Poisson)")
-    ap.add_argument("--serve-cells", default="63,511", help="cells per side of a request, log-uniform range")
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=6.0, help="requests per second (Poisson)")
+    ap.add_argument("--serve-cells", default="63,1023", help="cells per side of a request, log-uniform range")
     ap.add_argument("--serve-steps", default="1,20", help="timesteps per request, uniform range")
     ap.add_argument("--hbm-budget-gb", type=float, default=64.0)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="default line without the bounded precision / batch / serve forms object")
+    ap.add_argument("--forms-batch", type=int, default=64, help="forms object: batch instances")
+    ap.add_argument("--forms-requests", type=int, default=16, help="forms object: serve requests")
+    ap.add_argument("--forms-rate", type=float, default=4.0, help="forms object: serve requests per second")
+    ap.add_argument("--forms-cells", default="63,511", help="forms object: serve cells per side")
+    ap.add_argument("--forms-precision-n", type=int, default=1024, help="forms object: precision grid points")
+    ap.add_argument("--forms-precision-steps", type=int, default=3, help="forms object: precision timesteps")
     ap.add_argument("--fold-every", type=int, default=400)
     ap.add_argument("--tile-rows", type=int, default=0,
                     help="rows of the FP32 sweep tiles (8, 16, 32); 0: the autotuner chooses rows and schedule")
@@ -459,73 +468,99 @@ def _rel_l2(a, b):
     return d / n if n > 0 else d
 
 
-def run_precision_form(a):
+def _fields_l2(got, ref, names):
+    return {f: _rel_l2(got[f], ref[f]) for f in names}
+
+
+def _worst(rows, names):
+    return {f: max((r[f] for r in rows), default=None) for f in names}
+
+
+def run_precision_form(a, *, n=None, cases=None, steps=None, contrast=None):
     """Precision form: the plume timesteps of the default workload (n x n grid points, markers per cell as
     given) with the plume viscosity drawn from seed (matrix/plume contrast log-uniform over
-    10**precision_contrast), each timestep solved twice from the same deposited state: plain FP64 and FP32
-    sweeps + FP64 defect correction, both to relative residual rtol.  Reported per case: solve time of each
-    and the relative L2 distance of V and P between them after every timestep (both carry their own state
-    forward; markers advect with their own velocities)."""
+    10**contrast), each timestep solved by the plain FP64 path (the oracle) and by FP32 sweeps + FP64 defect
+    correction, both to relative residual rtol, each carrying its own state (V, P, damped rates, dt,
+    markers) forward.  Reported per timestep: solve time and iterations of each, and the relative L2
+    distance of V, P and the marker positions between them."""
     import numpy as np
     import stokesflow_b200 as sf
     torch.cuda.set_device(0)
+    n = n or a.n
+    cases = cases or a.precision_cases
+    steps = steps or a.precision_steps
+    contrast = contrast or a.precision_contrast
     rng = np.random.default_rng(a.seed)
-    lo, hi = _pair(a.precision_contrast)
+    lo, hi = _pair(contrast)
     md = sf.driver.marker_density_for(a.markers_per_cell)
     opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
                             tile_schedule=a.tile_schedule)
+    names = ("rel_l2_Vx", "rel_l2_Vy", "rel_l2_P", "rel_l2_markers_x", "rel_l2_markers_y")
     clocks = ClockSampler(0)
     clocks.start()
-    cases = []
-    for c in range(a.precision_cases):
-        contrast = float(10.0 ** rng.uniform(lo, hi))
+    out_cases = []
+    for c in range(cases):
+        C = float(10.0 ** rng.uniform(lo, hi))
         model = sf.plume_model_unit_square()
         model.mu_air = a.mu_air
-        model.mu_plume = model.mu_matrix / contrast
-        states = {s: sf.StokesFlow2D(a.n, a.n, 1.0, 1.0, model, marker_density=md, stokes_rtol=a.rtol, jitter=0.5,
+        model.mu_plume = model.mu_matrix / C
+        states = {s: sf.StokesFlow2D(n, n, 1.0, 1.0, model, marker_density=md, stokes_rtol=a.rtol, jitter=0.5,
                                      seed=0, iter_max=SOLVE_CAP, keep_work_arrays=False, solver=s, mixed_opts=opts)
                   for s in ("fp64", "mixed")}
-        steps = []
-        for k in range(a.precision_steps):
+        rows = []
+        for k in range(steps):
             rec = {s: st.step() for s, st in states.items()}
             f, m = states["fp64"], states["mixed"]
-            steps.append({"fp64_solve_ms": round(rec["fp64"]["times"].solve_ms, 2),
-                          "mixed_solve_ms": round(rec["mixed"]["times"].solve_ms, 2),
-                          "fp64_iters": int(rec["fp64"]["info"]["iters"]),
-                          "mixed_sweeps": int(rec["mixed"]["info"]["inner_iters"]),
-                          "rel_l2_Vx": _rel_l2(m.Vx, f.Vx), "rel_l2_Vy": _rel_l2(m.Vy, f.Vy),
-                          "rel_l2_P": _rel_l2(m.P, f.P), "rel_l2_markers_x": _rel_l2(m.x_m, f.x_m),
-                          "rel_l2_markers_y": _rel_l2(m.y_m, f.y_m)})
-        fs = sum(s["fp64_solve_ms"] for s in steps)
-        ms = sum(s["mixed_solve_ms"] for s in steps)
-        cases.append({"contrast": contrast, "mu_plume": model.mu_plume, "fp64_solve_ms_total": round(fs, 1),
-                      "mixed_solve_ms_total": round(ms, 1), "solve_speedup": round(fs / ms, 3), "steps": steps})
+            rows.append({"fp64_solve_ms": round(rec["fp64"]["times"].solve_ms, 2),
+                         "mixed_solve_ms": round(rec["mixed"]["times"].solve_ms, 2),
+                         "fp64_iters": int(rec["fp64"]["info"]["iters"]),
+                         "mixed_sweeps": int(rec["mixed"]["info"]["inner_iters"]),
+                         "rel_l2_Vx": _rel_l2(m.Vx, f.Vx), "rel_l2_Vy": _rel_l2(m.Vy, f.Vy),
+                         "rel_l2_P": _rel_l2(m.P, f.P), "rel_l2_markers_x": _rel_l2(m.x_m, f.x_m),
+                         "rel_l2_markers_y": _rel_l2(m.y_m, f.y_m)})
+        fs = sum(r["fp64_solve_ms"] for r in rows)
+        ms = sum(r["mixed_solve_ms"] for r in rows)
+        out_cases.append({"contrast": C, "mu_plume": model.mu_plume, "fp64_solve_ms_total": round(fs, 1),
+                          "mixed_solve_ms_total": round(ms, 1), "solve_speedup": round(fs / ms, 3),
+                          "same_iterations": all(r["fp64_iters"] == r["mixed_sweeps"] for r in rows), "steps": rows})
         del states
         torch.cuda.empty_cache()
     clk = clocks.stop()
-    worst = {k: max(s[k] for cs in cases for s in cs["steps"]) for k in ("rel_l2_Vx", "rel_l2_Vy", "rel_l2_P",
-                                                                       "rel_l2_markers_x", "rel_l2_markers_y")}
-    fs = sum(cs["fp64_solve_ms_total"] for cs in cases)
-    ms = sum(cs["mixed_solve_ms_total"] for cs in cases)
+    fs = sum(cs["fp64_solve_ms_total"] for cs in out_cases)
+    ms = sum(cs["mixed_solve_ms_total"] for cs in out_cases)
+    nsolves = cases * steps
     return {"form": "precision", "metric": f"solve time and rel L2 vs plain FP64, relative residual {a.rtol:g}",
-            "unit": "ms / rel L2", "solve_speedup": round(fs / ms, 3), "worst_rel_l2": worst, "cases": cases,
+            "unit": "ms / rel L2", "solves_per_s": round(nsolves / (ms * 1e-3), 4),
+            "fp64_solves_per_s": round(nsolves / (fs * 1e-3), 4), "solve_speedup": round(fs / ms, 3),
+            "max_rel_l2": _worst([r for cs in out_cases for r in cs["steps"]], names),
+            "same_iterations": all(cs["same_iterations"] for cs in out_cases), "cases": out_cases,
             "dtype": "f32 sweeps + f64 correction / f64", "data": "synthetic (seeded markers and contrasts)",
             "clocks": clk,
-            "config": {"workload": f"plume, {a.n - 1}x{a.n - 1} cells, {a.markers_per_cell} markers/cell, matrix/"
-                                   f"plume viscosity contrast log-uniform 10**[{a.precision_contrast}], "
-                                   f"{a.precision_steps} warm-started timesteps per case, air mu {a.mu_air:g}",
+            "config": {"workload": f"plume, {n - 1}x{n - 1} cells, {a.markers_per_cell} markers/cell, matrix/"
+                                   f"plume viscosity contrast log-uniform 10**[{contrast}], {steps} timesteps per "
+                                   f"case from a cold start, air mu {a.mu_air:g}",
+                       "oracle": "plain FP64 path (bit-identical to the reference) at the same tolerance",
                        "fold_every": a.fold_every, "seed": a.seed}}
 
 
-def run_batch_form(a):
+def run_batch_form(a, *, instances=None, cells=None, concurrency=None):
     """Batching form: N independent problems (seeded random grids and inclusion layouts) solved to relative
-    residual rtol in ONE engine run (FP32 sweeps + FP64 defect correction, one launch per sweep for all
-    instances, graph replay) against a loop of plain FP64 solves of the same problems."""
+    residual rtol in one resident engine (FP32 sweeps + FP64 defect correction, one launch per sweep for all
+    instances, graph replay, the tuner's sweep shapes) against the plain FP64 path on the same problems:
+    a loop of solves one after the other (the plain form as it is called), and, with concurrency K > 1, K
+    host threads each with its own context and stream, so that K plain solves share the GPU.  Every
+    instance's result is compared with its plain FP64 result (the oracle at the same tolerance).  Latency of
+    an instance: from the start of the run to its completion."""
+    import statistics as stats
+
     import stokesflow_b200 as sf
     from stokesflow_b200 import workloads
     torch.cuda.set_device(0)
-    specs = workloads.batch_specs(a.batch_instances, a.seed, cells=_pair(a.batch_cells, int),
-                                  mu_log10=_pair(a.mu_log10), mu_air=a.mu_air)
+    instances = instances or a.batch_instances
+    cells = cells or a.batch_cells
+    concurrency = a.fp64_concurrency if concurrency is None else concurrency
+    specs = workloads.batch_specs(instances, a.seed, cells=_pair(cells, int), mu_log10=_pair(a.mu_log10),
+                                  mu_air=a.mu_air)
     inst = _deposit_instances(sf, specs)
     opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
                             tile_schedule=a.tile_schedule)
@@ -538,17 +573,17 @@ def run_batch_form(a):
             arrs.append(s)
             probs.append(sf.MixedProblem(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"],
                                          s["Vx_s"], s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5,
-                                         rel_tol=a.rtol))
+                                         rel_tol=a.rtol, dVxdt=s["dVx"], dVydt=s["dVy"]))
         return probs, arrs
 
-    def fp64_solve(d, s, rtol=a.rtol):
+    def fp64_solve(d, s, ctx=None):
         sp = d["spec"]
-        scale = sf.residual_scale(d["rho_vy"], sp.Nx, sp.Ny, 9.81)
+        scale = sf.residual_scale(d["rho_vy"], sp.Nx, sp.Ny, 9.81, ctx=ctx)
         try:
             return sf.solve_stokes_info(s["P"], s["Vx_pad"], s["Vy_pad"], d["rho_vy"], d["mu_b"], d["mu_p"], None,
                                         None, None, None, None, None, None, s["dVx"], s["dVy"], None, None, s["Vx_s"],
                                         s["Vy_s"], 9.81, d["dx"], d["dy"], sp.Nx, sp.Ny, 0.0, 0.5,
-                                        eps=rtol * scale, iter_max=SOLVE_CAP)
+                                        eps=a.rtol * scale, iter_max=SOLVE_CAP, ctx=ctx)
         except sf.StokesFlowError as e:
             if e.status != 5:   # SF_ERR_NONFINITE: the instance diverged; anything else is an error
                 raise
@@ -560,79 +595,133 @@ def run_batch_form(a):
     for d in small:
         fp64_solve(d, _state_arrays(sf, d["spec"].Nx, d["spec"].Ny))
     probs, arrs = mixed_problems(inst)
-    k = a.fp64_sample if a.fp64_sample > 0 else len(inst)
-    fp64_arrs = [_state_arrays(sf, d["spec"].Nx, d["spec"].Ny) for d in inst[:k]]
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    arena = sum(sf.Engine.instance_bytes(d["spec"].Nx, d["spec"].Ny) for d in inst)
     clocks = ClockSampler(0)
     clocks.start()
-    e0.record()
-    res = sf.solve_stokes_batch_mixed(probs, options=opts)
-    e1.record()
+    # ---- the engine: every instance admitted at once, rounds until all have left ----
+    lat_m = [None] * len(inst)
+    with sf.Engine(arena, len(inst), options=opts) as eng:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pid = {id(p): q for q, p in enumerate(probs)}
+        for p in probs:
+            assert eng.submit(p) is not None
+        while eng.active:
+            for p in eng.step():
+                lat_m[pid[id(p)]] = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        mixed_s = time.perf_counter() - t0
+        tiles = eng.stats()
+    res = [p.result for p in probs]
+    # ---- plain FP64, one solve after the other ----
+    fp64_arrs = [_state_arrays(sf, d["spec"].Nx, d["spec"].Ny) for d in inst]
+    lat_f, infos = [], []
     torch.cuda.synchronize()
-    mixed_s = e0.elapsed_time(e1) / 1e3
-    tiles = sf.batch_stats()   # the last sweep choice; the tuner's trial pieces are inside the timed region
-    e0.record()
-    infos = [fp64_solve(d, s) for d, s in zip(inst[:k], fp64_arrs)]
-    e1.record()
-    torch.cuda.synchronize()
-    fp64_s = e0.elapsed_time(e1) / 1e3
+    t0 = time.perf_counter()
+    for d, s in zip(inst, fp64_arrs):
+        infos.append(fp64_solve(d, s))
+        lat_f.append(time.perf_counter() - t0)
+    fp64_s = time.perf_counter() - t0
+    # ---- plain FP64, K solves at a time ----
+    conc = None
+    if concurrency > 1:
+        conc_arrs = [_state_arrays(sf, d["spec"].Nx, d["spec"].Ny) for d in inst]
+        nxt = iter(range(len(inst)))
+        lock = threading.Lock()
+        lat_c = [None] * len(inst)
+        errs = []
+
+        def worker():
+            ctx = sf.Context(0)
+            try:
+                with torch.cuda.stream(torch.cuda.Stream()):
+                    while True:
+                        with lock:
+                            q = next(nxt, None)
+                        if q is None or errs:
+                            break
+                        fp64_solve(inst[q], conc_arrs[q], ctx)
+                        lat_c[q] = time.perf_counter() - t1
+            except BaseException as e:
+                errs.append(e)
+            finally:
+                torch.cuda.synchronize()
+                ctx.close()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        ths = [threading.Thread(target=worker) for _ in range(concurrency)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        if errs:
+            raise errs[0]
+        conc_s = time.perf_counter() - t1
+        conc = {"workers": concurrency, "solves_per_s": round(len(inst) / conc_s, 4), "s": round(conc_s, 3),
+                "p50_latency_s": round(stats.median(lat_c), 3),
+                "p99_latency_s": round(float(_percentile(lat_c, 99)), 3)}
+        del conc_arrs
     clk = clocks.stop()
-    errs = {f: sorted(_rel_l2(arrs[q][f], fp64_arrs[q][f]) for q in range(k)
-                      if res[q]["status"] == 0 and infos[q]["converged"]) for f in ("Vx_pad", "Vy_pad", "P")}
-    # both stopped at rtol are a convergence error away from the discrete solution: measure each against a
-    # tight FP64 solve (relative residual 1e-10) on the smallest timed instances
-    tight = []
-    for q in sorted(range(k), key=lambda q: inst[q]["spec"].points)[:8]:
-        if res[q]["status"] != 0 or not infos[q]["converged"]:
-            continue
-        d = inst[q]
-        t = _state_arrays(sf, d["spec"].Nx, d["spec"].Ny)
-        if not fp64_solve(d, t, rtol=1e-10)["converged"]:
-            continue
-        tight.append({"instance": q, "cells": [d["spec"].Nx - 1, d["spec"].Ny - 1],
-                      **{f"mixed_{f}": _rel_l2(arrs[q][f], t[f]) for f in ("Vx_pad", "Vy_pad", "P")},
-                      **{f"fp64_{f}": _rel_l2(fp64_arrs[q][f], t[f]) for f in ("Vx_pad", "Vy_pad", "P")}})
+    names = ("Vx_pad", "Vy_pad", "P")
+    ok = [q for q in range(len(inst)) if res[q]["status"] == 0 and infos[q]["converged"] and res[q]["converged"]]
+    l2 = [_fields_l2(arrs[q], fp64_arrs[q], names) for q in ok]
     pts = [d["spec"].points for d in inst]
     mixed_rate = len(inst) / mixed_s
-    fp64_rate = k / fp64_s
-    mixed_sweeps = sum(r["inner_iters"] for r in res)
-    return {"form": "batch", "metric": f"Stokes solves/s to relative residual {a.rtol:g}, independent instances",
-            "unit": "solves/s", "value": round(mixed_rate, 3), "fp64_loop_value": round(fp64_rate, 3),
-            "speedup_vs_fp64_loop": round(mixed_rate / fp64_rate, 3), "higher_is_better": True,
-            "mixed_s": round(mixed_s, 3), "fp64_s": round(fp64_s, 3), "fp64_instances_timed": k,
-            "instances": len(inst), "converged": sum(r["converged"] for r in res),
-            "nonfinite": sum(1 for r in res if r["status"] == 5),
-            "fp64_converged": sum(int(i["converged"]) for i in infos),
-            "fp64_nonfinite": sum(int(i.get("nonfinite", 0)) for i in infos),
-            "retried": sum(int(r.get("retried", 0)) for r in res),
-            "mixed_sweeps_total": int(mixed_sweeps), "fp64_iters_total": int(sum(i["iters"] for i in infos)),
-            "fp32_sweep_gpts": round(sum(r["inner_iters"] * pts[q] for q, r in enumerate(res)) / mixed_s / 1e9, 3),
-            "rel_l2_vs_fp64_same_rtol": {f: {"median": v[len(v) // 2] if v else None, "max": v[-1] if v else None}
-                                         for f, v in errs.items()},
-            "vs_tight_fp64": tight,
-            "nonfinite_instances": [q for q, r in enumerate(res) if r["status"] == 5],
-            "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"],
-                            "overlapped_launches": tiles["overlap_launches"], "tuner": tiles["tune_state"],
-                            "classes_measured": tiles["tune_rounds"], "classes_recalled": tiles["tune_hits"],
-                            "gpts_per_s_timed": {k: round(1.0 / v, 2) for k, v in tiles["tune_ns"].items() if v > 0}},
-            "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
-            "clocks": clk,
-            "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {a.batch_cells}, 9-25 "
-                                   f"markers/cell, 1-3 inclusions mu log10-uniform {a.mu_log10}, air mu "
-                                   f"{a.mu_air:g}", "grid_points_total": int(sum(pts)),
-                       "markers_total": int(sum(d['markers'] for d in inst)), "fold_every": a.fold_every,
-                       "seed": a.seed, "solve_cap": SOLVE_CAP}}
+    fp64_rate = len(inst) / fp64_s
+    out = {"form": "batch", "metric": f"Stokes solves/s to relative residual {a.rtol:g}, independent instances",
+           "unit": "solves/s", "solves_per_s": round(mixed_rate, 4), "fp64_loop_solves_per_s": round(fp64_rate, 4),
+           "speedup_solves_per_s": round(mixed_rate / fp64_rate, 3),
+           "p50_latency_s": round(stats.median(lat_m), 3), "p99_latency_s": round(float(_percentile(lat_m, 99)), 3),
+           "fp64_loop_p50_latency_s": round(stats.median(lat_f), 3),
+           "fp64_loop_p99_latency_s": round(float(_percentile(lat_f, 99)), 3),
+           "max_rel_l2": {f: max((x[f] for x in l2), default=None) for f in names},
+           "median_rel_l2": {f: (sorted(x[f] for x in l2)[len(l2) // 2] if l2 else None) for f in names},
+           "same_iterations": sum(1 for q in ok if res[q]["inner_iters"] == infos[q]["iters"]),
+           "compared": len(ok), "instances": len(inst),
+           "converged": sum(r["converged"] for r in res), "fp64_converged": sum(int(i["converged"]) for i in infos),
+           "nonfinite": sum(1 for r in res if r["status"] == 5),
+           "fp64_nonfinite": sum(int(i.get("nonfinite", 0)) for i in infos),
+           "retried": sum(int(r.get("retried", 0)) for r in res),
+           "mixed_s": round(mixed_s, 3), "fp64_loop_s": round(fp64_s, 3),
+           "mixed_sweeps_total": int(sum(r["inner_iters"] for r in res)),
+           "fp64_iters_total": int(sum(i["iters"] for i in infos)),
+           "fp32_sweep_gpts": round(sum(r["inner_iters"] * pts[q] for q, r in enumerate(res)) / mixed_s / 1e9, 3),
+           "sweep_tiles": {"rows": tiles["tile_rows"], "schedule": tiles["tile_schedule"],
+                           "overlapped_launches": tiles["overlap_launches"], "tuner": tiles["tune_state"],
+                           "classes_measured": tiles["tune_rounds"], "classes_recalled": tiles["tune_hits"]},
+           "dtype": "f32 sweeps + f64 correction", "data": "synthetic (seeded random inclusion layouts)",
+           "clocks": clk,
+           "config": {"workload": f"{len(inst)} instances, cells per side log-uniform {cells}, 9-25 "
+                                  f"markers/cell, 1-3 inclusions mu log10-uniform {a.mu_log10}, air mu "
+                                  f"{a.mu_air:g}", "grid_points_total": int(sum(pts)),
+                      "markers_total": int(sum(d['markers'] for d in inst)), "fold_every": a.fold_every,
+                      "oracle": "plain FP64 path (bit-identical to the reference) at the same tolerance",
+                      "seed": a.seed, "solve_cap": SOLVE_CAP}}
+    if conc is not None:
+        out["fp64_concurrent"] = conc
+        out["speedup_vs_fp64_concurrent"] = round(mixed_rate / conc["solves_per_s"], 3)
+    return out
 
 
-def run_serve_form(a):
+def _percentile(xs, q):
+    import numpy as np
+    return np.percentile(np.asarray(xs, dtype=np.float64), q)
+
+
+def run_serve_form(a, *, requests=None, rate=None, cells=None, concurrency=None):
     """Serving form: a Poisson stream of StokesFlow2D requests (1-20 timesteps each, random grids and
-    inclusion layouts), continuous batching through the resident engine against plain FP64 serving (one
-    request at a time, arrival order), on the same request trace."""
+    inclusion layouts), continuous batching through the resident engine against plain FP64 serving on the
+    same request trace: one request at a time in arrival order (the plain form as it is called), and, with
+    concurrency K > 1, K workers with their own contexts and streams.  Each mixed request's final state
+    (V, P, markers) is compared with the plain FP64 server's for the same request."""
     import stokesflow_b200 as sf
     from stokesflow_b200 import serving
     torch.cuda.set_device(0)
-    kw = dict(cells=_pair(a.serve_cells, int), timesteps=_pair(a.serve_steps, int), mu_log10=_pair(a.mu_log10),
+    requests = requests or a.serve_requests
+    rate = rate or a.serve_rate
+    cells = cells or a.serve_cells
+    concurrency = a.fp64_concurrency if concurrency is None else concurrency
+    kw = dict(cells=_pair(cells, int), timesteps=_pair(a.serve_steps, int), mu_log10=_pair(a.mu_log10),
               mu_air=a.mu_air)
     budget = int(a.hbm_budget_gb * 2 ** 30)
     opts = sf.mixed_options(max_sweeps=SOLVE_CAP, fold_every=a.fold_every, tile_rows=a.tile_rows,
@@ -645,28 +734,84 @@ def run_serve_form(a):
         srv.close()
     clocks = ClockSampler(0)
     clocks.start()
-    out = {}
-    for solver in ("mixed", "fp64"):
-        reqs = serving.poisson_requests(a.serve_requests, a.serve_rate, a.seed, **kw)
-        srv = serving.StokesServer(budget, solver=solver, rtol=a.rtol, options=opts, iter_max=SOLVE_CAP)
-        out[solver] = srv.run(reqs)
-        out[solver]["peak_state_bytes"] = srv.peak_state
+    out, finals = {}, {}
+    runs = [("mixed", 1), ("fp64", 1)] + ([("fp64", concurrency)] if concurrency > 1 else [])
+    for solver, k in runs:
+        key = solver if k == 1 else f"fp64_x{k}"
+        reqs = serving.poisson_requests(requests, rate, a.seed, **kw)
+        srv = serving.StokesServer(budget, solver=solver, rtol=a.rtol, options=opts, iter_max=SOLVE_CAP,
+                                   keep_final=(k == 1), concurrency=k)
+        out[key] = srv.run(reqs)
+        out[key]["peak_state_bytes"] = srv.peak_state
         if srv.engine is not None:
-            out[solver]["engine"] = srv.engine.stats()
+            out[key]["engine"] = srv.engine.stats()
         srv.close()
+        if k == 1:
+            finals[key] = {r.rid: r for r in reqs}
     clk = clocks.stop()
+    names = ("Vx", "Vy", "P", "x_m", "y_m")
+    l2 = []
+    for rid, rm in finals["mixed"].items():
+        rf = finals["fp64"][rid]
+        if rm.failed or rf.failed or rm.final is None or rf.final is None:
+            continue
+        l2.append({f: _rel_l2(torch.from_numpy(rm.final[f]), torch.from_numpy(rf.final[f])) for f in names})
     m, f = out["mixed"], out["fp64"]
-    return {"form": "serve", "metric": f"p50/p99 request latency and solves/s at relative residual {a.rtol:g}",
-            "unit": "s / solves/s", "p50_latency_s": round(m["p50_latency_s"], 4),
-            "p99_latency_s": round(m["p99_latency_s"], 4), "solves_per_s": round(m["solves_per_s"], 3),
-            "fp64_p50_latency_s": round(f["p50_latency_s"], 4), "fp64_p99_latency_s": round(f["p99_latency_s"], 4),
-            "fp64_solves_per_s": round(f["solves_per_s"], 3),
-            "speedup_solves_per_s": round(m["solves_per_s"] / f["solves_per_s"], 3),
-            "mixed": m, "fp64": f, "clocks": clk, "data": "synthetic (seeded Poisson trace, random inclusion layouts)",
-            "config": {"workload": f"{a.serve_requests} requests at {a.serve_rate:g}/s, square grids with cells per "
-                                   f"side log-uniform {a.serve_cells}, {a.serve_steps} timesteps, 9-25 markers/cell, "
-                                   f"inclusion mu log10-uniform {a.mu_log10}",
-                       "hbm_budget_bytes": budget, "fold_every": a.fold_every, "seed": a.seed}}
+    res = {"form": "serve", "metric": f"p50/p99 request latency and solves/s at relative residual {a.rtol:g}",
+           "unit": "s / solves/s", "solves_per_s": round(m["solves_per_s"], 3),
+           "p50_latency_s": round(m["p50_latency_s"], 4), "p99_latency_s": round(m["p99_latency_s"], 4),
+           "fp64_solves_per_s": round(f["solves_per_s"], 3), "fp64_p50_latency_s": round(f["p50_latency_s"], 4),
+           "fp64_p99_latency_s": round(f["p99_latency_s"], 4),
+           "speedup_solves_per_s": round(m["solves_per_s"] / f["solves_per_s"], 3),
+           "max_rel_l2": {k: max((x[k] for x in l2), default=None) for k in names},
+           "median_rel_l2": {k: (sorted(x[k] for x in l2)[len(l2) // 2] if l2 else None) for k in names},
+           "compared_requests": len(l2), "mixed": m, "fp64": f, "clocks": clk,
+           "data": "synthetic (seeded Poisson trace, random inclusion layouts)",
+           "config": {"workload": f"{requests} requests at {rate:g}/s, square grids with cells per side "
+                                  f"log-uniform {cells}, {a.serve_steps} timesteps, 9-25 markers/cell, inclusion "
+                                  f"mu log10-uniform {a.mu_log10}, air mu {a.mu_air:g}",
+                      "hbm_budget_bytes": budget, "fold_every": a.fold_every, "seed": a.seed,
+                      "oracle": "the plain FP64 server's final V, P and markers of the same request"}}
+    if concurrency > 1:
+        c = out[f"fp64_x{concurrency}"]
+        res["fp64_concurrent"] = {"workers": concurrency, "solves_per_s": round(c["solves_per_s"], 3),
+                                  "p50_latency_s": round(c["p50_latency_s"], 4),
+                                  "p99_latency_s": round(c["p99_latency_s"], 4)}
+        res["speedup_vs_fp64_concurrent"] = round(m["solves_per_s"] / c["solves_per_s"], 3)
+    return res
+
+
+def _brief(d, keys):
+    return {k: d[k] for k in keys if k in d}
+
+
+def run_forms(a):
+    """The three further forms, bounded so that they add a few minutes to the default run: a batch of
+    forms_batch instances of the batching workload with the full plain FP64 loop over the same instances, a
+    serve trace of forms_requests requests, and one precision case of forms_precision_n^2 grid points."""
+    forms = {}
+    t0 = time.perf_counter()
+    b = run_batch_form(a, instances=a.forms_batch, cells=a.batch_cells, concurrency=1)
+    forms["batch"] = _brief(b, ("solves_per_s", "fp64_loop_solves_per_s", "speedup_solves_per_s", "p50_latency_s",
+                                "p99_latency_s", "fp64_loop_p50_latency_s", "fp64_loop_p99_latency_s", "max_rel_l2",
+                                "median_rel_l2", "same_iterations", "compared", "instances", "converged",
+                                "fp64_converged", "clocks", "config"))
+    s = run_serve_form(a, requests=a.forms_requests, rate=a.forms_rate, cells=a.forms_cells, concurrency=1)
+    forms["serve"] = _brief(s, ("solves_per_s", "p50_latency_s", "p99_latency_s", "fp64_solves_per_s",
+                                "fp64_p50_latency_s", "fp64_p99_latency_s", "speedup_solves_per_s", "max_rel_l2",
+                                "median_rel_l2", "compared_requests", "clocks", "config"))
+    forms["serve"]["requests"] = s["mixed"]["requests"]
+    forms["serve"]["solves"] = s["mixed"]["solves"]
+    p = run_precision_form(a, n=a.forms_precision_n, cases=1, steps=a.forms_precision_steps,
+                           contrast=a.precision_contrast)
+    forms["precision"] = _brief(p, ("solves_per_s", "fp64_solves_per_s", "solve_speedup", "max_rel_l2",
+                                    "same_iterations", "clocks", "config"))
+    forms["precision"]["iterations"] = [[r["fp64_iters"], r["mixed_sweeps"]] for r in p["cases"][0]["steps"]]
+    forms["wall_s"] = round(time.perf_counter() - t0, 1)
+    forms["bar"] = {"rel_l2": 1e-5, "speedup_solves_per_s": 1.8,
+                    "note": "rel L2 of the FP32-with-correction result against the plain FP64 path (the oracle) at "
+                            "the same relative residual; speed-ups against the plain FP64 path on the same GPU"}
+    return forms
 
 
 def run_reference(a, rank):
@@ -727,6 +872,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
         out = run_ours(a, rank, world, local_rank)
+        if world == 1 and not a.no_forms:
+            out["forms"] = run_forms(a)
         if rank == 0:
             print(json.dumps(out), flush=True)
     finally:

@@ -291,11 +291,16 @@ typedef struct {
     int32_t status;            /* sf_status of this instance         */
     double batch_ms;           /* sf_solve_stokes_batch_mixed: device time of the whole batch;
                                   sf_engine: host time from submit to the step that finished it */
+    double* dVxdt;             /* (Nx-2, Ny-1) in/out, or NULL: the damped rates the solve starts from and
+                                  ends with, as solveStokes! keeps dVxdtau between calls (a timestep
+                                  loop passes the previous solve's); NULL starts them at zero and
+                                  returns nothing                                              */
+    double* dVydt;             /* (Nx-1, Ny-2) in/out, or NULL: likewise dVydtau               */
 } sf_batch_instance;
 
 typedef struct {
     int64_t max_sweeps;        /* FP32 sweeps per instance at most (4,000,000)                         */
-    int32_t fold_every;        /* FP32 sweeps between folds into the FP64 state, even (400)            */
+    int32_t fold_every;        /* FP32 sweeps between folds into the FP64 state at most, even (400)    */
     int32_t use_graphs;        /* replay the sweeps between folds from a captured CUDA graph (1)       */
     int32_t dtau_local_max;    /* 1: pseudo-time step of a velocity node from the largest viscosity of
                                   its stencil (both pressure cells, both shear nodes), which converges
@@ -337,23 +342,34 @@ enum {
 
 /* Solves n independent Stokes problems (each as in solveStokes!, with its own
  * grid size) to err <= eps by FP64 defect correction around FP32
- * pseudo-transient sweeps.  Every fold_every sweeps the FP32 correction is
- * added to the FP64 V and P, dt is recomputed from them (compute_dt) and the
- * FP64 residual is evaluated -- that is the stopping test and the constant
- * term of the next sweeps.  The sweeps are the reference's PT iteration
- * (damping, pseudo-time steps, free-slip BCs) on the correction; its damped
- * rates carry over across folds, so in exact arithmetic the sequence is the
- * FP64 iteration itself.  One sweep of every instance still iterating is a
- * single kernel launch over a shared tile list.  opt may be NULL (defaults
- * above).  Synchronises the stream.  The results are FP32-accurate
- * corrections of an FP64 solution, not bit-identical to sf_solve_stokes. */
+ * pseudo-transient sweeps.  At most every fold_every sweeps the FP32
+ * correction is added to the FP64 V and P and the FP64 residual of the sum is
+ * evaluated: the constant term of the next sweeps.  The sweeps are the
+ * reference's PT iteration (damping, pseudo-time steps, free-slip BCs) on the
+ * correction; its damped rates carry over across folds, so in exact arithmetic
+ * the sequence is the FP64 iteration itself.  The solve keeps the reference
+ * loop's schedule (StokesSolver_multixpu.jl:43-77): the stabilisation dt is the
+ * one passed in until iteration ndtupdate = 10 min(Nx, Ny) and is recomputed
+ * (compute_dt) at every multiple of it; the residual check (compute_Residuals!
+ * with dt_check, compute_err) runs at every multiple of ncheck = min(5 min(Nx,
+ * Ny), 2000) on the same quantities as the reference's, and the solve stops at
+ * the first check with err <= eps or after max_sweeps iterations -- so it stops
+ * at the same iteration as sf_solve_stokes on the same inputs, apart from a
+ * check whose err lies within FP32 rounding of eps.  One sweep of every
+ * instance still iterating is a single kernel launch over a shared tile list.
+ * opt may be NULL (defaults above).  Synchronises the stream.  The results are
+ * FP32-accurate corrections of an FP64 solution, not bit-identical to
+ * sf_solve_stokes. */
 int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst, int n, const sf_mixed_options* opt,
                                 void* stream);
 
 /* One problem through the batch path; info (may be NULL) receives the
- * per-instance results. */
+ * per-instance results.  dVxdt (Nx-2, Ny-1) and dVydt (Nx-1, Ny-2) are the
+ * damped rates, in/out as in solveStokes!; either may be NULL (start at zero,
+ * nothing returned). */
 int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy,
-                          const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s, double g_y,
+                          const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s, double* dVxdt,
+                          double* dVydt, double g_y,
                           double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
                           int use_free_surface_stabilization, double eps, double rel_tol,
                           const sf_mixed_options* opt, void* stream, sf_batch_instance* info);
@@ -365,10 +381,11 @@ int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad
  * that instances can join and leave while others iterate.  It owns a device
  * arena of arena_bytes (the HBM budget of its solves) and a table of at most
  * max_instances instances.  Each sf_engine_step is one round: every admitted
- * instance folds its correction, gets its FP64 residual and stopping test;
- * the finished ones are written back to their caller arrays and leave (arena
- * space and table slot free at once); the rest run fold_every FP32 sweeps
- * (one launch per sweep over all of them, graph-replayed).  An instance's
+ * instance folds its correction and gets its FP64 residual (and, where its
+ * schedule has one, its dt update and residual check); the finished ones are
+ * written back to their caller arrays and leave (arena space and table slot
+ * free at once); the rest run up to fold_every FP32 sweeps, each up to its
+ * next event (one launch per sweep over all of them, graph-replayed).  An instance's
  * arithmetic and stopping decisions depend on itself alone, so its results
  * are bit-identical whatever else is in the engine and whenever it joined. */
 typedef struct sf_engine sf_engine;

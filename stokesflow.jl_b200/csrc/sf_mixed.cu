@@ -91,11 +91,20 @@ struct Inst {  // device-side description of one instance
     int64_t fstride32, fstride64;
     float _dxf, _dyf, dampXf, dampYf, c_vscf, c_ptscf;   // FP32 constants
     float g_dtf;            // g_y * dt for the stabilisation term of the correction
-    int parity;             // which dV/dP buffer is "in" at launch parity 0
+    int pad1_;
     double dx, dy, _dx, _dy, g_y, dt, dt_cfl, dt_in, maxdisp;
     int use_stab;
     int dtau_max;           // pseudo-time step from the stencil's largest viscosity
 };
+
+// Per-instance control word, written by host copies between rounds only (never by a kernel):
+//   parity  which correction buffer (0: A, 1: B) holds the current correction before the round's first sweep;
+//   budget  sweeps the instance runs in this round: it sweeps in launches 0 .. budget-1 of the round and
+//           sits out the rest, so that every round ends exactly where the reference's loop has an event
+//           (a dt update every ndtupdate iterations, a residual check every ncheck, iterMax);
+//   flags   the events at the end of that round (CTL_DT, CTL_CHECK), read by the FP64 kernels of the next.
+struct Ctl { int parity, budget, flags, pad_; };
+enum { CTL_DT = 1, CTL_CHECK = 2 };
 
 __device__ __forceinline__ float* gf(const Inst& I, int k) { return I.f32 + (int64_t)k * I.fstride32; }
 __device__ __forceinline__ double* gd(const Inst& I, int k) { return I.f64 + (int64_t)k * I.fstride64; }
@@ -105,10 +114,14 @@ __device__ __forceinline__ double* gd(const Inst& I, int k) { return I.f64 + (in
 // ---------------------------------------------------------------------------
 // The arithmetic of a point does not depend on BY: the file is compiled without contraction and the fused
 // multiply-adds below are written out, so every shape (and a change of shape between sweeps) gives the same bits.
+// Launch `launch_idx` of a round sweeps the tiles of the instances whose budget exceeds it; the others' tiles
+// are passed over without a copy.
 template <int BY, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict__ maps, const Inst* __restrict__ insts,
-                                                   const int2* __restrict__ tiles, const int* __restrict__ ntiles_ptr,
-                                                   int launch_parity, int chunked, int* __restrict__ err_flag) {
+                                                   const Ctl* __restrict__ ctl, const int2* __restrict__ tiles,
+                                                   const int* __restrict__ ntiles_ptr, int launch_idx, int chunked,
+                                                   int* __restrict__ err_flag) {
+    static_assert(NST == 2, "the copy pipeline runs one tile ahead");
     using S = Shape<BY>;
     constexpr int TH = S::TH, H1 = S::H1, RPT = S::RPT, HALO_BYTES = S::HALO_BYTES, TILE_BYTES = S::TILE_BYTES;
     constexpr int STAGE_BYTES = S::STAGE_BYTES, ST1_BYTES = S::ST1_BYTES;
@@ -137,6 +150,13 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         step = G;
         end = ntiles;
     }
+    // the tiles this CTA sweeps in this launch: its share of the list, less those of instances whose budget is
+    // used up (every thread walks the same sequence; control words and tile list are host-written)
+    auto next_live = [&](int t) {
+        for (; t < end; t += step)
+            if (ctl[tiles[t].x].budget > launch_idx) break;
+        return t;
+    };
     // the tile list is ordered by instance, so a CTA meets each instance in one run of tiles: the two maps it
     // reads are fenced when the run starts
     int fenced = -1;
@@ -145,22 +165,25 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         fence_tensormap_acquire(maps + (int64_t)x * M_NUM + M_TILE);
         fenced = x;
     };
+    int t = next_live(first);
     if (tid == 0) {
         for (int k = 0; k < NST; ++k) mbar_init(&bar[k], 1);
         fence_mbar_init();
         // the first instance's maps are fenced before the wait below, while the previous sweep may still run:
-        // maps, tile list and tile count are written by host copies before the sweeps, never by a sweep
-        if (first < end) fence_maps(tiles[first].x);
+        // maps, tile list, tile count and control words are written by host copies before the sweeps, never
+        // by a sweep
+        if (t < end) fence_maps(tiles[t].x);
     }
     __syncthreads();
     // the previous sweep's corrections and rates are complete and visible from here on
     griddep_wait();
     griddep_launch_dependents();
+    const int launch_parity = launch_idx & 1;
     auto issue = [&](int t, int s) {  // thread 0 only
         const int2 td = tiles[t];
         const Inst& I = insts[td.x];
         const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
-        const int in = (I.parity ^ launch_parity) & 1;
+        const int in = (ctl[td.x].parity ^ launch_parity) & 1;
         const CUtensorMap* H = maps + (int64_t)td.x * M_NUM + M_HALO;
         const CUtensorMap* T = maps + (int64_t)td.x * M_NUM + M_TILE;
         if (td.x != fenced) fence_maps(td.x);
@@ -179,29 +202,22 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         tma_load_3d(tb + 2 * TILE_BYTES, T, &bar[s], i0, j0, G_RX);
         tma_load_3d(tb + 3 * TILE_BYTES, T, &bar[s], i0, j0, G_RY);
     };
-    int t = first;
-    if (tid == 0)
-        for (int k = 0; k < NST - 1; ++k)
-            if (t + k * step < end) issue(t + k * step, k);
+    if (tid == 0 && t < end) issue(t, 0);
+    int tn = (t < end) ? next_live(t + step) : end;   // the tile after t, copied while t is computed
     uint32_t phase = 0;
     int s = 0;
     // a copy never completed: flag it, give every copy still in flight a bounded chance to land (the issuing
-    // thread knows their phases), leave together
+    // thread knows their phases: stage s has just been waited on, stage s^1 holds tile tn), leave together
     auto give_up = [&]() {
         if (tid == 0) {
             atomicExch(err_flag, 1);
-            for (int k = 0; k < NST; ++k) {
-                if (t + k * step >= end) break;
-                const int sk = (s + k) % NST;
-                const uint32_t par = (k == 0) ? (((phase >> sk) & 1u) ^ 1u) : ((phase >> sk) & 1u);
-                mbar_wait(&bar[sk], par, WAIT_BUDGET_NS);
-            }
+            mbar_wait(&bar[s], ((phase >> s) & 1u) ^ 1u, WAIT_BUDGET_NS);
+            if (tn < end) mbar_wait(&bar[s ^ 1], (phase >> (s ^ 1)) & 1u, WAIT_BUDGET_NS);
         }
         __syncthreads();
     };
-    for (; t < end; t += step) {
-        const int tn = t + (NST - 1) * step;
-        if (tid == 0 && tn < end) issue(tn, (s + NST - 1) % NST);
+    for (; t < end; t = tn, tn = (tn < end) ? next_live(tn + step) : end) {
+        if (tid == 0 && tn < end) issue(tn, s ^ 1);
         // the timeout vote rides on the stage-1 barrier below: stage 1 writes shared memory only, so a thread
         // whose copy did not land computes garbage there and nothing else before everyone leaves
         const bool ok = mbar_wait(&bar[s], (phase >> s) & 1u, WAIT_BUDGET_NS);
@@ -210,7 +226,7 @@ __global__ void __launch_bounds__(NT, MINB) k_pt32(const CUtensorMap* __restrict
         const Inst& I = insts[td.x];
         const int Nx = I.Nx, Ny = I.Ny;
         const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY;
-        const int in = (I.parity ^ launch_parity) & 1;
+        const int in = (ctl[td.x].parity ^ launch_parity) & 1;
         const int64_t LD = I.LD32;
         const float _dx = I._dxf, _dy = I._dyf;
         unsigned char* st = smem + s * STAGE_BYTES;
@@ -380,20 +396,25 @@ __device__ __forceinline__ double blk_max(double v, double* sh) {
     return r;
 }
 
-// max |Vx|, |Vy| of the FP64 state per tile (compute_dt's maxima; ghost entries repeat interior values or are 0)
-__global__ void __launch_bounds__(T64) k_maxv64(const Inst* __restrict__ insts, const int2* __restrict__ tiles,
-                                               double* __restrict__ part) {
+// max |Vx|, |Vy| per tile of V = V64 + correction, the velocity the next fold stores (compute_dt's maxima;
+// ghost entries repeat interior values or are 0).  Before an instance's first sweeps the correction is zero.
+__global__ void __launch_bounds__(T64) k_maxv64(const Inst* __restrict__ insts, const Ctl* __restrict__ ctl,
+                                               const int2* __restrict__ tiles, double* __restrict__ part) {
     __shared__ double sh[T64 / 32];
     const int2 td = tiles[blockIdx.x];
     const Inst& I = insts[td.x];
     const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY64;
     const double* Vx = gd(I, D_VX);
     const double* Vy = gd(I, D_VY);
+    const int cur = ctl[td.x].parity & 1;
+    const float* cvx = gf(I, cur ? G_VXB : G_VXA);
+    const float* cvy = gf(I, cur ? G_VYB : G_VYA);
     double mx = 0.0, my = 0.0;
     for (int k = threadIdx.x; k < BX * BY64; k += T64) {
         const int i = i0 + (k % BX), j = j0 + (k / BX);
-        if (i < I.Nx - 2 && j < I.Ny - 1) mx = fmax(mx, fabs(Vx[(i + 1) + (int64_t)(j + 1) * I.LD64]));
-        if (i < I.Nx - 1 && j < I.Ny - 2) my = fmax(my, fabs(Vy[(i + 1) + (int64_t)(j + 1) * I.LD64]));
+        const int64_t o = (i + 1) + (int64_t)(j + 1) * I.LD64;
+        if (i < I.Nx - 2 && j < I.Ny - 1) mx = fmax(mx, fabs(Vx[o] + (double)cvx[o]));
+        if (i < I.Nx - 1 && j < I.Ny - 2) my = fmax(my, fabs(Vy[o] + (double)cvy[o]));
     }
     double a = blk_max(mx, sh), b = blk_max(my, sh);
     if (threadIdx.x == 0) {
@@ -480,10 +501,104 @@ __global__ void __launch_bounds__(T64) k_resid64(const Inst* __restrict__ insts,
     }
 }
 
+// The residual check of the reference's loop at an iteration n that is a multiple of ncheck (:64-73, kernels
+// :140-202 and :241-249), evaluated before the fold from the FP64 state plus the two correction buffers:
+// divV and tau are those of compute_P_tau! in iteration n, i.e. of V_{n-1} (= V64 + the previous correction);
+// P is P_n (= P64 + the current correction); the stabilisation term of Ry uses V_n and dt_check =
+// compute_dt(V_n) (Inst::dt_cfl, computed just before).  Per-tile sums of |Rx|, |Ry|, |divV| -> part.  Tiles of
+// instances without a check this round leave at once.
+__global__ void __launch_bounds__(T64) k_check64(const Inst* __restrict__ insts, const Ctl* __restrict__ ctl,
+                                                const int2* __restrict__ tiles, double* __restrict__ part) {
+    __shared__ double sh[T64 / 32];
+    const int2 td = tiles[blockIdx.x];
+    const Ctl c = ctl[td.x];
+    if (!(c.flags & CTL_CHECK)) return;
+    const Inst& I = insts[td.x];
+    const int Nx = I.Nx, Ny = I.Ny;
+    const int i0 = (td.y % I.ntx) * BX, j0 = (td.y / I.ntx) * BY64;
+    const int64_t L = I.LD64;
+    const double* Vx = gd(I, D_VX);
+    const double* Vy = gd(I, D_VY);
+    const double* P = gd(I, D_P);
+    const double* rho = gd(I, D_RHO);
+    const double* mub = gd(I, D_MUB);
+    const double* mup = gd(I, D_MUP);
+    const int cur = c.parity & 1;
+    const float* cvx = gf(I, cur ? G_VXB : G_VXA);
+    const float* cvy = gf(I, cur ? G_VYB : G_VYA);
+    const float* cp = gf(I, cur ? G_PB : G_PA);
+    const float* pvx = gf(I, cur ? G_VXA : G_VXB);
+    const float* pvy = gf(I, cur ? G_VYA : G_VYB);
+    const double _dx = I._dx, _dy = I._dy;
+    const double dt = I.use_stab ? I.dt_cfl : 0.0;
+    // V_{n-1}, V_n and P_n at an offset (the FP32 and FP64 fields share i + j * LD)
+    auto vxp = [&](int64_t o) { return Vx[o] + (double)pvx[o]; };
+    auto vyp = [&](int64_t o) { return Vy[o] + (double)pvy[o]; };
+    auto vxc = [&](int64_t o) { return Vx[o] + (double)cvx[o]; };
+    auto vyc = [&](int64_t o) { return Vy[o] + (double)cvy[o]; };
+    auto pc = [&](int64_t o) { return P[o] + (double)cp[o]; };
+    auto div_at = [&](int i, int j, double* dvx, double* dvy) {
+        *dvx = (vxp((i + 1) + (int64_t)(j + 1) * L) - vxp(i + (int64_t)(j + 1) * L)) * _dx;
+        *dvy = (vyp((i + 1) + (int64_t)(j + 1) * L) - vyp((i + 1) + (int64_t)j * L)) * _dy;
+        return *dvx + *dvy;
+    };
+    auto txx_at = [&](int i, int j, double* tyy) {
+        double dVx_dx, dVy_dy;
+        const double d = div_at(i, j, &dVx_dx, &dVy_dy);
+        const double mu = mup[i + (int64_t)j * L];
+        *tyy = 2.0 * mu * (dVy_dy - 1.0 / 3.0 * d);
+        return 2.0 * mu * (dVx_dx - 1.0 / 3.0 * d);
+    };
+    auto txy_at = [&](int i, int j) {
+        const double dVx_dy = (vxp(i + (int64_t)(j + 1) * L) - vxp(i + (int64_t)j * L)) * _dy;
+        const double dVy_dx = (vyp((i + 1) + (int64_t)j * L) - vyp(i + (int64_t)j * L)) * _dx;
+        return 2.0 * mub[i + (int64_t)j * L] * 0.5 * (dVx_dy + dVy_dx);
+    };
+    double srx = 0.0, sry = 0.0, sdv = 0.0;
+    for (int k = threadIdx.x; k < BX * BY64; k += T64) {
+        const int i = i0 + (k % BX), j = j0 + (k / BX);
+        if (i >= Nx - 1 || j >= Ny - 1) continue;
+        const int64_t o = i + (int64_t)j * L;
+        double dvx, dvy, tyy0;
+        sdv += fabs(div_at(i, j, &dvx, &dvy));
+        const double txx0 = txx_at(i, j, &tyy0);
+        if (i < Nx - 2) {
+            double tyy1;
+            const double txx1 = txx_at(i + 1, j, &tyy1);
+            const double R = (txx1 - txx0) * _dx + (txy_at(i + 1, j + 1) - txy_at(i + 1, j)) * _dy -
+                             (pc(o + 1) - pc(o)) * _dx;
+            srx += fabs(R);
+        }
+        if (j < Ny - 2) {
+            double tyy1;
+            (void)txx_at(i, j + 1, &tyy1);
+            const double av = 0.25 * (vxc(i + (int64_t)(j + 1) * L) + vxc((i + 1) + (int64_t)(j + 1) * L) +
+                                      vxc(i + (int64_t)(j + 2) * L) + vxc((i + 1) + (int64_t)(j + 2) * L));
+            const double dxr = rho[(i + 2) + (int64_t)(j + 1) * L] - rho[i + (int64_t)(j + 1) * L];
+            const double dyr = rho[(i + 1) + (int64_t)(j + 2) * L] - rho[(i + 1) + (int64_t)j * L];
+            const double R = (tyy1 - tyy0) * _dy + (txy_at(i + 1, j + 1) - txy_at(i, j + 1)) * _dx -
+                             (pc(o + L) - pc(o)) * _dy +
+                             I.g_y * (rho[(i + 1) + (int64_t)(j + 1) * L] -
+                                      dt * (av * dxr * 0.5 * _dx + vyc((i + 1) + (int64_t)(j + 1) * L) * dyr * 0.5 * _dy));
+            sry += fabs(R);
+        }
+    }
+    double a = blk_sum(srx, sh), b = blk_sum(sry, sh), cc = blk_sum(sdv, sh);
+    if (threadIdx.x == 0) {
+        part[3 * blockIdx.x] = a;
+        part[3 * blockIdx.x + 1] = b;
+        part[3 * blockIdx.x + 2] = cc;
+    }
+}
+
 // per-instance reductions over the instance's contiguous range of tile partials
 struct Seg { int inst, begin, end, pad_; };
 
-__global__ void k_inst_dt(Inst* __restrict__ insts, const Seg* __restrict__ segs, const double* __restrict__ part) {
+// compute_dt (:118-121) of the velocity the fold stores -> Inst::dt_cfl (the check's dt_check and the solve's
+// returned dt); at an ndtupdate event (:60-62) it also becomes the stabilisation dt of the iterations that
+// follow.  The reference keeps the dt it was called with until then.
+__global__ void k_inst_dt(Inst* __restrict__ insts, const Ctl* __restrict__ ctl, const Seg* __restrict__ segs,
+                          const double* __restrict__ part) {
     __shared__ double sh[32];
     const Seg g = segs[blockIdx.x];
     double mx = 0.0, my = 0.0;
@@ -493,59 +608,71 @@ __global__ void k_inst_dt(Inst* __restrict__ insts, const Seg* __restrict__ segs
     }
     double a = blk_max(mx, sh), b = blk_max(my, sh);
     if (threadIdx.x == 0) {
-        // compute_dt (:118-121); while V is still zero the CFL dt is infinite and the stabilisation keeps
-        // the dt the solve started with (the reference's first dt update comes only once V is non-zero)
         Inst& I = insts[g.inst];
         double x = I.dx / a, y = I.dy / b;
         double m = (y < x) ? y : x;
         if (x != x) m = x;
         if (y != y) m = y;
         I.dt_cfl = I.maxdisp * m;
-        I.dt = I.use_stab ? (isfinite(I.dt_cfl) ? I.dt_cfl : I.dt_in) : 0.0;
-        I.g_dtf = (float)(I.g_y * I.dt);
+        // while V is exactly zero the CFL dt is infinite: the stabilisation then keeps its dt
+        if ((ctl[g.inst].flags & CTL_DT) && I.use_stab && isfinite(I.dt_cfl)) {
+            I.dt = I.dt_cfl;
+            I.g_dtf = (float)(I.g_y * I.dt);
+        }
     }
 }
 
-// per instance of the round: {err, residual scale, dt_cfl} -> out[3 q ..]
-__global__ void k_inst_err(const Seg* __restrict__ segs, const double* __restrict__ part, const Inst* __restrict__ insts,
-                           const double* __restrict__ scale, double* __restrict__ out) {
+// err = max of the three means (compute_err, :103-109) of a sum triple
+__device__ __forceinline__ double err_of(const Inst& I, double a, double b, double c) {
+    const double nrx = (double)(I.Nx - 2) * (I.Ny - 1), nry = (double)(I.Nx - 1) * (I.Ny - 2),
+                 ndv = (double)(I.Nx - 1) * (I.Ny - 1);
+    double m = a / nrx;
+    const double bb = b / nry, cc = c / ndv;
+    if (bb > m || bb != bb) m = bb;
+    if (cc > m || cc != cc) m = cc;
+    if (a != a) m = a;
+    return m;
+}
+
+// per instance of the round -> out[4 q ..] = {err of the folded state (its residual, which is the constant term of
+// the next sweeps; a non-finite value ends the solve), residual scale, dt_cfl, err of the reference's check (when
+// the round ended on one, else 0)}
+__global__ void k_inst_err(const Seg* __restrict__ segs, const double* __restrict__ part,
+                           const double* __restrict__ part_check, const Inst* __restrict__ insts,
+                           const Ctl* __restrict__ ctl, const double* __restrict__ scale, double* __restrict__ out) {
     __shared__ double sh[32];
     const Seg g = segs[blockIdx.x];
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int t = g.begin + threadIdx.x; t < g.end; t += blockDim.x) {
-        s0 += part[3 * t];
-        s1 += part[3 * t + 1];
-        s2 += part[3 * t + 2];
-    }
-    double a = blk_sum(s0, sh), b = blk_sum(s1, sh), c = blk_sum(s2, sh);
+    const bool check = (ctl[g.inst].flags & CTL_CHECK) != 0;
+    double s[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int t = g.begin + threadIdx.x; t < g.end; t += blockDim.x)
+        for (int k = 0; k < 3; ++k) {
+            s[k] += part[3 * t + k];
+            if (check) s[3 + k] += part_check[3 * t + k];
+        }
+    double r[6];
+    for (int k = 0; k < 6; ++k) r[k] = blk_sum(s[k], sh);
     if (threadIdx.x == 0) {
         const Inst& I = insts[g.inst];
-        double nrx = (double)(I.Nx - 2) * (I.Ny - 1), nry = (double)(I.Nx - 1) * (I.Ny - 2),
-               ndv = (double)(I.Nx - 1) * (I.Ny - 1);
-        double m = a / nrx;
-        double bb = b / nry, cc = c / ndv;
-        if (bb > m || bb != bb) m = bb;
-        if (cc > m || cc != cc) m = cc;
-        if (a != a) m = a;
-        out[3 * blockIdx.x] = m;
-        out[3 * blockIdx.x + 1] = scale[g.inst];
-        out[3 * blockIdx.x + 2] = I.dt_cfl;
+        out[4 * blockIdx.x] = err_of(I, r[0], r[1], r[2]);
+        out[4 * blockIdx.x + 1] = scale[g.inst];
+        out[4 * blockIdx.x + 2] = I.dt_cfl;
+        out[4 * blockIdx.x + 3] = check ? err_of(I, r[3], r[4], r[5]) : 0.0;
     }
 }
 
 // V += dV, P += dP (FP64 += FP32) over an instance's padded arrays, then zero the correction.  The damped
 // rates are kept: folding the correction into the FP64 state and re-anchoring the constant term on the FP64
 // residual leaves the PT iteration itself unchanged (in exact arithmetic it is the FP64 iteration), so its
-// accumulated momentum stays valid.  blockIdx.y = position in the instance list.
-__global__ void k_accumulate(const Inst* __restrict__ insts, const int* __restrict__ list, int launch_parity) {
-    const Inst& I = insts[list[blockIdx.y]];
-    const int in = (I.parity ^ launch_parity) & 1;
+// accumulated momentum stays valid.  The other correction buffer (the previous iterate's) is left as it is:
+// the next sweep overwrites it.  blockIdx.y = position in the instance list.
+__global__ void k_accumulate(const Inst* __restrict__ insts, const Ctl* __restrict__ ctl, const int* __restrict__ list) {
+    const int q = list[blockIdx.y];
+    const Inst& I = insts[q];
+    const int cur = ctl[q].parity & 1;
     const int64_t n = I.LD32 * I.rows;  // every entry; the FP64 and FP32 fields share (i, j) -> i + j*LD
-    float* cvx = gf(I, in ? G_VXB : G_VXA);
-    float* cvy = gf(I, in ? G_VYB : G_VYA);
-    float* cp = gf(I, in ? G_PB : G_PA);
-    float* rvx = gf(I, G_RVX);
-    float* rvy = gf(I, G_RVY);
+    float* cvx = gf(I, cur ? G_VXB : G_VXA);
+    float* cvy = gf(I, cur ? G_VYB : G_VYA);
+    float* cp = gf(I, cur ? G_PB : G_PA);
     double* Vx = gd(I, D_VX);
     double* Vy = gd(I, D_VY);
     double* P = gd(I, D_P);
@@ -558,8 +685,15 @@ __global__ void k_accumulate(const Inst* __restrict__ insts, const int* __restri
         cvy[k] = 0.f;
         cp[k] = 0.f;
     }
-    (void)rvx;
-    (void)rvy;
+}
+
+__global__ void k_f32_to_f64(double* __restrict__ dst, int64_t ld_dst, const float* __restrict__ src, int64_t ld_src,
+                             int64_t nx, int64_t ny) {
+    int64_t n = nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = k % nx, j = k / nx;
+        dst[i + j * ld_dst] = (double)src[i + j * ld_src];
+    }
 }
 
 __global__ void k_f64_to_f32(float* __restrict__ dst, int64_t ld_dst, const double* __restrict__ src, int64_t ld_src,
@@ -620,7 +754,7 @@ static unsigned grid1(int64_t n, int per) { return (unsigned)std::max<int64_t>(1
 
 // The sweep shapes the autotuner chooses from: tile rows, and the CTAs per SM that the register budget is
 // sized for (the shared memory of a CTA grows with the rows: 31, 56 and 105 KB).
-typedef void (*SweepKernel)(const CUtensorMap*, const Inst*, const int2*, const int*, int, int, int*);
+typedef void (*SweepKernel)(const CUtensorMap*, const Inst*, const Ctl*, const int2*, const int*, int, int, int*);
 struct SweepShape {
     int rows, minb, smem;
     SweepKernel kern;
@@ -734,8 +868,10 @@ struct Slot {  // an admitted instance
     int64_t off = 0, bytes = 0;
     bool active = false;
     bool swept = false;        // ran sweeps since its last fold
+    int budget = 0;            // sweeps of its last round
+    int64_t ncheck = 0, ndtupdate = 0;   // the reference's event periods for this grid (:35-36)
     int64_t inner_total = 0, outer = 0;
-    double err = 0.0, eps = 0.0;
+    double err = 0.0, eps = 0.0;   // err of the last residual check (2 eps before the first, as :40)
     std::chrono::steady_clock::time_point t_submit;
 };
 
@@ -754,7 +890,7 @@ static sf_mixed_options normalized(const sf_mixed_options* o) {
         r.overlap_launches = 0;
     }
     if (r.fold_every < 2) r.fold_every = 2;
-    r.fold_every &= ~1;  // even: the current correction is back in the A buffers at every fold
+    r.fold_every &= ~1;  // even: the trial pieces of the tuner run in pairs of sweeps
     return r;
 }
 
@@ -773,9 +909,11 @@ struct sf_engine {
     ArenaAlloc alloc;
     std::vector<Slot> slots;
     std::vector<int> free_slots;
-    // device tables, one allocation: insts | maps | segs | out | scale | list | ntiles | flag
+    // device tables, one allocation: insts | ctl | maps | segs | out | scale | list | ntiles | flag
     void* tables = nullptr;
     Inst* d_insts = nullptr;
+    Ctl* d_ctl = nullptr;                // per-slot control words, uploaded from h_ctl before the kernels read them
+    std::vector<Ctl> h_ctl;
     CUtensorMap* d_maps = nullptr;       // [shape][slot][M_NUM]: every slot's maps for every shape
     Seg* d_segs = nullptr;
     double* d_out = nullptr;
@@ -788,7 +926,8 @@ struct sf_engine {
     int2* d_tiles[NSHAPES] = {};         // one sweep list per shape (tile counts differ)
     int64_t tile_cap[NSHAPES] = {};
     int2* d_tiles64 = nullptr;
-    double* d_part = nullptr;
+    double* d_part = nullptr;            // 3 per tile: max|V| pairs, then the folded residual's sums ...
+    double* d_part_check = nullptr;      // ... and 3 per tile for the check's sums (same allocation)
     int64_t tile64_cap = 0;
     std::vector<int2> h_tiles;
     std::vector<Seg> h_segs;
@@ -864,10 +1003,11 @@ int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options*
     SF_CUDA(cudaEventCreateWithFlags(&e->ev_out, cudaEventDisableTiming));
     for (cudaEvent_t& ev : e->ev_piece) SF_CUDA(cudaEventCreate(&ev));
     const size_t n = (size_t)slot_cap;
-    const size_t o_ins = 0, o_map = round_up(o_ins + n * sizeof(Inst), 256);
+    const size_t o_ins = 0, o_ctl = round_up(o_ins + n * sizeof(Inst), 256);
+    const size_t o_map = round_up(o_ctl + n * sizeof(Ctl), 256);
     const size_t o_seg = round_up(o_map + (size_t)NSHAPES * n * M_NUM * sizeof(CUtensorMap), 256);
     const size_t o_out = round_up(o_seg + n * sizeof(Seg), 256);
-    const size_t o_scl = round_up(o_out + n * 3 * 8, 256);
+    const size_t o_scl = round_up(o_out + n * 4 * 8, 256);
     const size_t o_lst = round_up(o_scl + n * 8, 256);
     const size_t o_nt = round_up(o_lst + n * 4, 256);
     const size_t o_flg = o_nt + 128;
@@ -878,6 +1018,7 @@ int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options*
     }
     unsigned char* b = (unsigned char*)e->tables;
     e->d_insts = (Inst*)(b + o_ins);
+    e->d_ctl = (Ctl*)(b + o_ctl);
     e->d_maps = (CUtensorMap*)(b + o_map);
     e->d_segs = (Seg*)(b + o_seg);
     e->d_out = (double*)(b + o_out);
@@ -886,14 +1027,15 @@ int engine_init(sf_engine* e, sf_ctx* ctx, int slot_cap, const sf_mixed_options*
     e->d_ntiles = (int*)(b + o_nt);
     e->d_flag = (int*)(b + o_flg);
     SF_CUDA(cudaMemsetAsync(e->tables, 0, total, e->s));
-    SF_CUDA(cudaMallocHost(&e->h_out, n * 3 * 8 + 64));  // {err, scale, dt_cfl} per slot, then the flag word
+    SF_CUDA(cudaMallocHost(&e->h_out, n * 4 * 8 + 64));  // 4 results per slot (k_inst_err), then the flag word
     e->slots.assign(n, Slot{});
+    e->h_ctl.assign(n, Ctl{0, 0, 0, 0});
     e->free_slots.clear();
     for (int k = slot_cap - 1; k >= 0; --k) e->free_slots.push_back(k);
     return configure_tuner(e);
 }
 
-// grows a device tile list (and, for the FP64 list, its per-tile partials)
+// grows a device tile list (and, for the FP64 list, its per-tile partials: 6 per tile)
 int grow_list(sf_engine* e, int64_t need, int2** tiles, double** part, int64_t* cap_io) {
     if (need <= *cap_io) return SF_OK;
     const int64_t cap = std::max<int64_t>({need, 2 * *cap_io, 4096});
@@ -904,7 +1046,7 @@ int grow_list(sf_engine* e, int64_t need, int2** tiles, double** part, int64_t* 
     if (part) *part = nullptr;
     *cap_io = 0;
     if (cudaMalloc(tiles, (size_t)cap * sizeof(int2)) != cudaSuccess ||
-        (part && cudaMalloc(part, (size_t)cap * 3 * 8) != cudaSuccess)) {
+        (part && cudaMalloc(part, (size_t)cap * 6 * 8) != cudaSuccess)) {
         cudaGetLastError();
         return fail(SF_ERR_OOM, "sf_engine: tile list");
     }
@@ -919,6 +1061,7 @@ int upload_lists64(sf_engine* e, const std::vector<int>& ids, int64_t* nt_out) {
     for (int q : ids) nt += e->slots[q].ntiles64;
     int rc = grow_list(e, nt, &e->d_tiles64, &e->d_part, &e->tile64_cap);
     if (rc) return rc;
+    e->d_part_check = e->d_part + 3 * e->tile64_cap;
     e->h_segs.resize(ids.size());
     int64_t k = 0;
     for (size_t q = 0; q < ids.size(); ++q) {
@@ -1043,25 +1186,29 @@ int tuner_collect(sf_engine* e) {
     return use_cand(e, best);
 }
 
-// `n` sweeps (launch parities k0, k0 + 1, ...) over the uploaded sweep list of the current shape
+// `n` sweeps (launch indices k0, k0 + 1, ... of the round) over the uploaded sweep list of the current shape
 int launch_direct(sf_engine* e, int k0, int n) {
     const int sk = e->shape;
     const SweepShape& sh = kShapes[sk];
     // overlapped: each sweep may launch while the previous one drains; it waits in the kernel for its results
     for (int k = k0; k < k0 + n; ++k)
         SF_CUDA(launch_overlapped(e->overlap != 0, sh.kern, dim3(e->blocks), dim3(BX, TY), (size_t)sh.smem, e->s,
-                                  maps_of(e, sk), (const Inst*)e->d_insts, (const int2*)e->d_tiles[sk],
-                                  (const int*)(e->d_ntiles + sk), k & 1, e->sched, e->d_flag));
+                                  maps_of(e, sk), (const Inst*)e->d_insts, (const Ctl*)e->d_ctl,
+                                  (const int2*)e->d_tiles[sk], (const int*)(e->d_ntiles + sk), k, e->sched,
+                                  e->d_flag));
     return SF_OK;
 }
 
 // a measuring round: its first sweeps run as short timed pieces, one per trial still to run (P sweeps each, P
 // even so that the launch parities run on), the rest in the default candidate; all launched directly, after
-// the lists of every shape are uploaded, so that nothing but sweeps lies between the events
+// the lists of every shape are uploaded, so that nothing but sweeps lies between the events.  The pieces stay
+// within the smallest budget of the round, so each covers every instance of the set.
 int launch_trials(sf_engine* e, const std::vector<int>& ids, double points) {
     const int K = e->opt.fold_every;
     const int P = std::min(8, std::max(2, (K / (2 * NCAND)) & ~1));
-    const int pieces = std::min(NCAND * TUNE_PASSES - e->tune_trials, K / P);
+    int min_budget = K;
+    for (int q : ids) min_budget = std::min(min_budget, e->slots[q].budget);
+    const int pieces = std::min(NCAND * TUNE_PASSES - e->tune_trials, min_budget / P);
     const int prev = cand_of(e->shape, e->sched, e->overlap);
     int rc, k = 0;
     ++e->tune_rounds;
@@ -1194,6 +1341,23 @@ int admit(sf_engine* e, int q, sf_batch_instance& u, int dtau_max) {
                                                              f64 + (int64_t)c.d * I.fstride64, LD, c.nx, c.ny);
         SF_LAUNCHED(ctx);
     }
+    // the damped rates the solve starts from: the caller's (solveStokes! keeps dVxdtau, dVydtau from one call
+    // to the next), or zero; rate (i, j) sits at the offset of point (i, j)
+    struct Rt { int g; const double* src; int64_t nx, ny; } rts[] = {{G_RVX, u.dVxdt, Nx - 2, Ny - 1},
+                                                                     {G_RVY, u.dVydt, Nx - 1, Ny - 2}};
+    for (const Rt& r : rts) {
+        if (!r.src) continue;
+        k_f64_to_f32<<<grid1(r.nx * r.ny, 256), 256, 0, s>>>(I.f32 + (int64_t)r.g * I.fstride32, LD, r.src, r.nx,
+                                                             r.nx, r.ny);
+        SF_LAUNCHED(ctx);
+    }
+    // the reference's event periods (:35-36; nx_g, ny_g are the grid's own on one domain); the correction
+    // starts in the A buffers, no sweeps yet
+    const int64_t mn = std::min(Nx, Ny);
+    h.ncheck = std::min<int64_t>(5 * mn, 2000);
+    h.ndtupdate = 10 * mn;
+    h.budget = 0;
+    e->h_ctl[q] = Ctl{0, 0, 0, 0};
     if (u.rel_tol > 0) {
         k_rho_scale64<<<1, 1024, 0, s>>>(u.rho_vy, (int)Nx, (int)Ny, u.g_y, e->d_scale + q);
         SF_LAUNCHED(ctx);
@@ -1216,6 +1380,14 @@ int write_back(sf_engine* e, int q, double dt_cfl) {
         {u.Vx_s, D_VX, Nx, Ny + 1}, {u.Vy_s, D_VY, Nx + 1, Ny}, {u.P, D_P, Nx - 1, Ny - 1}};
     for (const Uk& k : ups) {
         k_copy64<<<grid1(k.nx * k.ny, 256), 256, 0, s>>>(k.dst, k.nx, I.f64 + (int64_t)k.f * I.fstride64, LD, k.nx, k.ny);
+        SF_LAUNCHED(ctx);
+    }
+    struct Rt { double* dst; int g; int64_t nx, ny; } rts[] = {{u.dVxdt, G_RVX, Nx - 2, Ny - 1},
+                                                               {u.dVydt, G_RVY, Nx - 1, Ny - 2}};
+    for (const Rt& r : rts) {
+        if (!r.dst) continue;
+        k_f32_to_f64<<<grid1(r.nx * r.ny, 256), 256, 0, s>>>(r.dst, r.nx, I.f32 + (int64_t)r.g * I.fstride32, LD, r.nx,
+                                                             r.ny);
         SF_LAUNCHED(ctx);
     }
     k_pad_vx64<<<grid1((Nx + 2) * (Ny + 1), 256), 256, 0, s>>>(u.Vx_pad, I.f64 + D_VX * I.fstride64, LD, (int)Nx, (int)Ny);
@@ -1276,60 +1448,93 @@ int engine_submit(sf_engine* e, sf_batch_instance* u, cudaStream_t caller, int64
     return SF_OK;
 }
 
-// one round: fold -> dt -> FP64 residual -> stopping test -> write-back of the finished -> sweeps of the rest
+// one round: [max|V| -> dt -> the reference's check where one is due] -> fold -> FP64 residual -> stopping test ->
+// write-back of the finished -> sweeps of the rest.  Each instance's rounds end exactly on its iterations
+// with an event in the reference's loop (:43-77): a dt update every ndtupdate iterations, a residual check
+// every ncheck, iterMax; a round of fold_every sweeps is cut short for an instance whose next event comes
+// sooner (its budget), so the sequence of dt values, the checks and the iteration it stops at are the FP64
+// solver's.
 int engine_round(sf_engine* e, cudaStream_t caller) {
     sf_ctx* ctx = e->ctx;
     cudaStream_t s = e->s;
     std::vector<int> ids, swept;
+    bool any_check = false;
     for (int q = 0; q < (int)e->slots.size(); ++q)
         if (e->slots[q].active) {
             ids.push_back(q);
-            if (e->slots[q].swept) swept.push_back(q);
+            Slot& h = e->slots[q];
+            if (h.swept) {
+                swept.push_back(q);
+                // an odd budget leaves the current correction in the other buffer
+                if (h.budget & 1) e->h_ctl[q].parity ^= 1;
+                any_check = any_check || (e->h_ctl[q].flags & CTL_CHECK);
+            }
         }
     if (ids.empty()) return SF_OK;
     ++e->rounds;
     int rc;
-    if (!swept.empty()) {  // V += dV, P += dP for every instance that ran sweeps
-        SF_CUDA(cudaMemcpyAsync(e->d_list, swept.data(), swept.size() * 4, cudaMemcpyHostToDevice, s));
-        k_accumulate<<<dim3(64, (unsigned)swept.size()), 256, 0, s>>>(e->d_insts, e->d_list, 0);
-        SF_LAUNCHED(ctx);
-    }
+    // pageable source: staged before the call returns
+    SF_CUDA(cudaMemcpyAsync(e->d_ctl, e->h_ctl.data(), e->h_ctl.size() * sizeof(Ctl), cudaMemcpyHostToDevice, s));
     int64_t nt = 0;
     if ((rc = upload_lists64(e, ids, &nt))) return rc;
-    k_maxv64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles64, e->d_part);
+    k_maxv64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_ctl, e->d_tiles64, e->d_part);
     SF_LAUNCHED(ctx);
-    k_inst_dt<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_insts, e->d_segs, e->d_part);
+    k_inst_dt<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_insts, e->d_ctl, e->d_segs, e->d_part);
     SF_LAUNCHED(ctx);
+    if (any_check) {
+        k_check64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_ctl, e->d_tiles64, e->d_part_check);
+        SF_LAUNCHED(ctx);
+    }
+    if (!swept.empty()) {  // V += dV, P += dP for every instance that ran sweeps
+        SF_CUDA(cudaMemcpyAsync(e->d_list, swept.data(), swept.size() * 4, cudaMemcpyHostToDevice, s));
+        k_accumulate<<<dim3(64, (unsigned)swept.size()), 256, 0, s>>>(e->d_insts, e->d_ctl, e->d_list);
+        SF_LAUNCHED(ctx);
+    }
     k_resid64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles64, e->d_part);
     SF_LAUNCHED(ctx);
-    k_inst_err<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_segs, e->d_part, e->d_insts, e->d_scale, e->d_out);
+    k_inst_err<<<(unsigned)ids.size(), 256, 0, s>>>(e->d_segs, e->d_part, e->d_part_check, e->d_insts, e->d_ctl,
+                                                    e->d_scale, e->d_out);
     SF_LAUNCHED(ctx);
-    SF_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, ids.size() * 3 * 8, cudaMemcpyDeviceToHost, s));
-    SF_CUDA(cudaMemcpyAsync(e->h_out + ids.size() * 3, e->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(e->h_out, e->d_out, ids.size() * 4 * 8, cudaMemcpyDeviceToHost, s));
+    SF_CUDA(cudaMemcpyAsync(e->h_out + ids.size() * 4, e->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     SF_CUDA(cudaStreamSynchronize(s));
     int flag = 0;
-    memcpy(&flag, e->h_out + ids.size() * 3, sizeof(int));
+    memcpy(&flag, e->h_out + ids.size() * 4, sizeof(int));
     if (flag) return fail(SF_ERR_CUDA, "sf_engine: a tile copy did not complete in time");
     if ((rc = tuner_collect(e))) return rc;
+    const int K = e->opt.fold_every;
+    const int64_t max_sweeps = e->opt.max_sweeps;
     std::vector<int> sweep;
     bool any_done = false;
     for (size_t k = 0; k < ids.size(); ++k) {
         const int q = ids[k];
         Slot& h = e->slots[q];
-        h.err = e->h_out[3 * k];
-        if (h.outer == 0) h.eps = h.user->rel_tol > 0 ? h.user->rel_tol * e->h_out[3 * k + 1] : h.user->eps;
+        Ctl& c = e->h_ctl[q];
+        const double err_fold = e->h_out[4 * k];
+        if (h.outer == 0) {
+            h.eps = h.user->rel_tol > 0 ? h.user->rel_tol * e->h_out[4 * k + 1] : h.user->eps;
+            h.err = 2.0 * h.eps;  // :40, before the first check
+        }
         ++h.outer;
+        const bool at_check = (c.flags & CTL_CHECK) != 0;
+        if (at_check) h.err = e->h_out[4 * k + 3];
         h.swept = false;
-        const bool bad = !(h.err == h.err) || std::isinf(h.err);
-        if (bad && e->opt.retry_local_max && !h.d.dtau_max && h.inner_total < e->opt.max_sweeps) {
+        c.flags = 0;
+        const bool bad = !(err_fold == err_fold) || std::isinf(err_fold) || !(h.err == h.err) || std::isinf(h.err);
+        if (bad && e->opt.retry_local_max && !h.d.dtau_max && h.inner_total < max_sweeps) {
             // restart from the caller's inputs (untouched until write-back) with the stencil-maximum
-            // pseudo-time step; it re-enters with the next round's residual, its sweeps keep counting
+            // pseudo-time step; its sweeps keep counting, the first check comes after ncheck more
+            const int64_t done = h.inner_total, outer = h.outer;
             if ((rc = admit(e, q, *h.user, 1))) return rc;
+            h.inner_total = done;
+            h.outer = outer;
+            h.err = 2.0 * h.eps;
             h.user->retried = 1;
             continue;
         }
-        if (bad || h.err <= h.eps || h.inner_total >= e->opt.max_sweeps) {
-            if ((rc = write_back(e, q, e->h_out[3 * k + 2]))) return rc;
+        if (bad) h.err = (h.err == h.err && !std::isinf(h.err)) ? err_fold : h.err;
+        if (bad || (at_check && h.err <= h.eps) || h.inner_total >= max_sweeps) {
+            if ((rc = write_back(e, q, e->h_out[4 * k + 2]))) return rc;
             h.active = false;
             e->alloc.release(h.off, h.bytes);
             e->free_slots.push_back(q);
@@ -1345,9 +1550,25 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
         SF_CUDA(cudaStreamWaitEvent(caller, e->ev_out, 0));
     }
     if (sweep.empty()) return SF_OK;
+    // budgets: up to the next event of each instance (relative iteration counts; a restarted instance keeps
+    // counting), at most fold_every
+    for (int q : sweep) {
+        Slot& h = e->slots[q];
+        Ctl& c = e->h_ctl[q];
+        const int64_t it = h.inner_total;
+        int64_t b = std::min<int64_t>(K, h.ncheck - it % h.ncheck);
+        const bool stab = h.d.use_stab != 0;
+        if (stab) b = std::min<int64_t>(b, h.ndtupdate - it % h.ndtupdate);
+        b = std::max<int64_t>(1, std::min<int64_t>(b, max_sweeps - it));
+        const int64_t end = it + b;
+        c.budget = (int)b;
+        c.flags = ((end % h.ncheck == 0) ? CTL_CHECK : 0) | ((stab && end % h.ndtupdate == 0) ? CTL_DT : 0);
+        h.budget = (int)b;
+    }
+    SF_CUDA(cudaMemcpyAsync(e->d_ctl, e->h_ctl.data(), e->h_ctl.size() * sizeof(Ctl), cudaMemcpyHostToDevice, s));
     if ((rc = launch_sweeps(e, sweep))) return rc;
     for (int q : sweep) {
-        e->slots[q].inner_total += e->opt.fold_every;
+        e->slots[q].inner_total += e->slots[q].budget;
         e->slots[q].swept = true;
     }
     return SF_OK;
@@ -1515,7 +1736,8 @@ extern "C" int sf_solve_stokes_batch_mixed(sf_ctx* ctx, sf_batch_instance* inst,
     return SF_OK;
 }
 extern "C" int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, double* Vy_pad, const double* rho_vy,
-                                     const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s, double g_y,
+                                     const double* mu_b, const double* mu_p, double* Vx_s, double* Vy_s,
+                                     double* dVxdt, double* dVydt, double g_y,
                                      double dx, double dy, int64_t Nx, int64_t Ny, double dt, double maxdisp,
                                      int use_stab, double eps, double rel_tol, const sf_mixed_options* opt,
                                      void* stream, sf_batch_instance* info) {
@@ -1529,6 +1751,8 @@ extern "C" int sf_solve_stokes_mixed(sf_ctx* ctx, double* P, double* Vx_pad, dou
     u.mu_p = mu_p;
     u.Vx_s = Vx_s;
     u.Vy_s = Vy_s;
+    u.dVxdt = dVxdt;
+    u.dVydt = dVydt;
     u.Nx = Nx;
     u.Ny = Ny;
     u.g_y = g_y;

@@ -100,20 +100,23 @@ struct BatchInstance
     inner_iters::Int64; outer_iters::Int64
     converged::Int32; status::Int32
     batch_ms::Float64
+    dVxdt::Ptr{Cdouble}; dVydt::Ptr{Cdouble}
 end
 
 # The problem of solveStokes! solved by FP32 pseudo-transient sweeps with FP64 defect correction: the same
-# FP64 stopping test, not the same bits.  Returns (dt, err, FP32 sweeps).  rel_tol > 0 replaces ϵ by
+# FP64 stopping test and iteration schedule, not the same bits.  dVxdτ, dVydτ are the damped rates, carried
+# from call to call as solveStokes! carries them.  Returns (dt, err, FP32 sweeps).  rel_tol > 0 replaces ϵ by
 # rel_tol * mean|g_y ρ_vy|.
-function solveStokesMixed!(P, Vx_pad, Vy_pad, ρ_vy, μ_b, μ_p, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp;
-                           use_free_surface_stabilization::Bool=true, ϵ=1e-8, rel_tol=0.0)
+function solveStokesMixed!(P, Vx_pad, Vy_pad, ρ_vy, μ_b, μ_p, Vx_s, Vy_s, dVxdτ, dVydτ, g_y, dx, dy, Nx, Ny, dt,
+                           maxdisp; use_free_surface_stabilization::Bool=true, ϵ=1e-8, rel_tol=0.0)
     info = Ref{BatchInstance}()
     check(ccall((:sf_solve_stokes_mixed, libsf), Cint,
                 (Ptr{Cvoid}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble},
-                 Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Cdouble, Cdouble, Int64, Int64, Cdouble, Cdouble, Cint, Cdouble,
-                 Cdouble, Ptr{Cvoid}, Ptr{Cvoid}, Ref{BatchInstance}),
+                 Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Cdouble, Cdouble, Cdouble, Int64, Int64,
+                 Cdouble, Cdouble, Cint, Cdouble, Cdouble, Ptr{Cvoid}, Ptr{Cvoid}, Ref{BatchInstance}),
                 ctx(), dptr(P), dptr(Vx_pad), dptr(Vy_pad), dptr(ρ_vy), dptr(μ_b), dptr(μ_p), dptr(Vx_s), dptr(Vy_s),
-                g_y, dx, dy, Nx, Ny, dt, maxdisp, use_free_surface_stabilization, ϵ, rel_tol, C_NULL, stream(), info))
+                dptr(dVxdτ), dptr(dVydτ), g_y, dx, dy, Nx, Ny, dt, maxdisp, use_free_surface_stabilization, ϵ,
+                rel_tol, C_NULL, stream(), info))
     return info[].dt_out, info[].err, info[].inner_iters
 end
 

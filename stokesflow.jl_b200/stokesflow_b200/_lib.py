@@ -64,7 +64,7 @@ class BatchInstance(C.Structure):
                 ("dt", _d), ("maxdisp", _d), ("eps", _d), ("rel_tol", _d),
                 ("use_free_surface_stabilization", _i32), ("retried", _i32), ("dt_out", _d), ("err", _d),
                 ("eps_used", _d), ("inner_iters", _i64), ("outer_iters", _i64), ("converged", _i32),
-                ("status", _i32), ("batch_ms", _d)]
+                ("status", _i32), ("batch_ms", _d), ("dVxdt", _vp), ("dVydt", _vp)]
 
     RESULTS = ("dt_out", "err", "eps_used", "inner_iters", "outer_iters", "converged", "status", "batch_ms",
                "retried")
@@ -146,7 +146,8 @@ PROTOTYPES = {
     "sf_safe_division": (C.c_int, [_vp, _pd, _i64, _i64, _pd, _pd, _i64, _vp]),
     "sf_exchange_markers": (C.c_int, [C.POINTER(MarkerRank), _i32, _i32, _d, _d, _d, _d]),
     "sf_solve_stokes_batch_mixed": (C.c_int, [_vp, C.POINTER(BatchInstance), C.c_int, C.POINTER(MixedOptions), _vp]),
-    "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64, _d, _d,
+    "sf_solve_stokes_mixed": (C.c_int, [_vp, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _d, _d, _d, _i64, _i64,
+                                        _d, _d,
                                         C.c_int, _d, _d, C.POINTER(MixedOptions), _vp, C.POINTER(BatchInstance)]),
     "sf_engine_instance_bytes": (C.c_int, [_i64, _i64, C.POINTER(_i64)]),
     "sf_engine_create": (C.c_int, [_vp, _i64, _i32, C.POINTER(MixedOptions), C.POINTER(_vp)]),

@@ -209,11 +209,12 @@ def solve_stokes(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtP
 class MixedProblem:
     """One Stokes problem for the mixed-precision / batched solver: the caller arrays of
     :func:`solve_stokes` (state in/out) and its scalars.  ``eps`` is absolute; ``rel_tol`` > 0
-    replaces it by rel_tol * mean|g_y rho_vy|.  After a solve, ``result`` holds dt_out, err,
-    inner/outer iteration counts and the convergence flag."""
+    replaces it by rel_tol * mean|g_y rho_vy|.  ``dVxdt``, ``dVydt`` (optional, in/out) are the damped
+    rates that solveStokes! keeps from one call to the next; without them the solve starts them at zero.
+    After a solve, ``result`` holds dt_out, err, inner/outer iteration counts and the convergence flag."""
 
     def __init__(self, P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, Vx_s, Vy_s, g_y, dx, dy, Nx, Ny, dt, maxdisp,
-                 eps=1e-8, rel_tol=0.0, use_free_surface_stabilization=True):
+                 eps=1e-8, rel_tol=0.0, use_free_surface_stabilization=True, dVxdt=None, dVydt=None):
         Nx, Ny = int(Nx), int(Ny)
         self.arrays = dict(P=P, Vx_pad=Vx_pad, Vy_pad=Vy_pad, rho_vy=rho_vy, mu_b=mu_b, mu_p=mu_p, Vx_s=Vx_s,
                            Vy_s=Vy_s)
@@ -222,6 +223,12 @@ class MixedProblem:
         c = _lib.BatchInstance()
         for k, a in self.arrays.items():
             setattr(c, k, _grid(a, k, shapes[k]))
+        c.dVxdt = _opt_grid(dVxdt, "dVxdt", (Nx - 2, Ny - 1))
+        c.dVydt = _opt_grid(dVydt, "dVydt", (Nx - 1, Ny - 2))
+        if dVxdt is not None:
+            self.arrays["dVxdt"] = dVxdt
+        if dVydt is not None:
+            self.arrays["dVydt"] = dVydt
         c.Nx, c.Ny = Nx, Ny
         c.g_y, c.dx, c.dy, c.dt, c.maxdisp = float(g_y), float(dx), float(dy), float(dt), float(maxdisp)
         c.eps, c.rel_tol = float(eps), float(rel_tol)

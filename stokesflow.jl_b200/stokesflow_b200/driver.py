@@ -157,7 +157,8 @@ class StokesFlow2D:
         """This timestep's Stokes problem for the mixed-precision / batched solver."""
         return api.MixedProblem(self.P, self.Vx, self.Vy, self.rho_vy, self.mu_b, self.mu_p, self.Vx_s, self.Vy_s,
                                 self.g_y, self.dx, self.dy, self.Nx, self.Ny, self.dt, self.maxdisp,
-                                eps=self.stokes_eps, rel_tol=self.stokes_rtol or 0.0)
+                                eps=self.stokes_eps, rel_tol=self.stokes_rtol or 0.0, dVxdt=self.dVxdt,
+                                dVydt=self.dVydt)
 
     def solve(self):
         if self.solver == "mixed":

@@ -14,14 +14,18 @@ Two servers over the same request trace:
   one engine round; a request whose solve converged in it advects, deposits
   its next timestep and re-enters the engine at once, while newly admitted
   requests join between rounds -- no request waits for a batch to drain.
-* ``solver="fp64"``: the plain path, one request at a time in arrival order,
-  each timestep a blocking ``solveStokes!`` (bit-identical to the reference).
+* ``solver="fp64"``: the plain path, each timestep a blocking ``solveStokes!``
+  (bit-identical to the reference).  With ``concurrency=1`` one request at a
+  time in arrival order; with ``concurrency=K`` K worker threads, each with its
+  own context and CUDA stream, take requests in arrival order, so up to K
+  plain solves share the GPU (HBM admission as for the mixed server).
 
 Latency of a request = completion time - arrival time.
 """
 from __future__ import annotations
 
 import math
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass
@@ -94,10 +98,13 @@ class StokesServer:
 
     def __init__(self, hbm_budget: int, *, solver: str = "mixed", rtol: float = 1e-6, options=None,
                  max_instances: int = 1024, engine_share: float = 0.5, iter_max: int = 4_000_000,
-                 keep_final: bool = False, ctx: api.Context | None = None):
+                 keep_final: bool = False, concurrency: int = 1, ctx: api.Context | None = None):
         if solver not in ("mixed", "fp64"):
             raise ValueError("solver must be 'mixed' or 'fp64'")
+        if concurrency < 1 or (concurrency > 1 and solver != "fp64"):
+            raise ValueError("concurrency: a positive worker count, for the fp64 server")
         self.solver = solver
+        self.concurrency = int(concurrency)
         self.rtol = rtol
         self.iter_max = iter_max
         self.keep_final = keep_final
@@ -118,11 +125,11 @@ class StokesServer:
             self.engine = None
 
     # ------------------------------------------------------------------
-    def _new_state(self, r: Request) -> StokesFlow2D:
+    def _new_state(self, r: Request, ctx: api.Context | None = None) -> StokesFlow2D:
         s = r.spec
         return StokesFlow2D(s.Nx, s.Ny, 1.0, 1.0, s.model, marker_density=s.md, stokes_rtol=self.rtol, jitter=0.5,
                             seed=s.seed, keep_work_arrays=False, solver=self.solver, iter_max=self.iter_max,
-                            ctx=self.ctx)
+                            ctx=ctx or self.ctx)
 
     def _finish(self, r: Request, now: float):
         r.t_done = now
@@ -141,6 +148,8 @@ class StokesServer:
         t0 = time.perf_counter()
         if self.solver == "mixed":
             self._run_mixed(pending, t0)
+        elif self.concurrency > 1:
+            self._run_fp64_concurrent(pending, t0)
         else:
             self._run_fp64(pending, t0)
         return summarize(requests)
@@ -206,6 +215,23 @@ class StokesServer:
             elif pending and not queue and not waiting:
                 time.sleep(max(0.0, pending[0].arrival - (time.perf_counter() - t0)))
 
+    def _serve_fp64(self, r: Request, ctx: api.Context | None = None):
+        """All timesteps of request r with the plain path, on the calling thread's current stream."""
+        r.state = self._new_state(r, ctx)
+        for _ in range(r.timesteps):
+            r.solves += 1
+            try:
+                rec = r.state.step()
+            except StokesFlowError as e:
+                if e.status != 5:   # SF_ERR_NONFINITE ends the request; anything else is an error
+                    raise
+                r.failed = True
+                break
+            info = rec["info"]
+            r.converged += int(info["converged"])
+            r.sweeps += int(info["iters"])
+        torch.cuda.current_stream().synchronize()
+
     def _run_fp64(self, pending: deque, t0: float):
         while pending:
             r = pending.popleft()
@@ -217,21 +243,62 @@ class StokesServer:
             r.state_bytes = state_bytes(r.spec)
             self.state_used = r.state_bytes
             self.peak_state = max(self.peak_state, self.state_used)
-            r.state = self._new_state(r)
-            for _ in range(r.timesteps):
-                r.solves += 1
-                try:
-                    rec = r.state.step()
-                except StokesFlowError as e:
-                    if e.status != 5:   # SF_ERR_NONFINITE ends the request; anything else is an error
-                        raise
-                    r.failed = True
-                    break
-                info = rec["info"]
-                r.converged += int(info["converged"])
-                r.sweeps += int(info["iters"])
-            torch.cuda.current_stream().synchronize()
+            self._serve_fp64(r)
             self._finish(r, time.perf_counter() - t0)
+
+    def _run_fp64_concurrent(self, pending: deque, t0: float):
+        """K workers, each with its own context and stream; a worker takes the next request in arrival order
+        once it has arrived and its state fits what the HBM budget has left."""
+        lock = threading.Condition()
+        errors = []
+        device = torch.cuda.current_device()
+
+        def next_request():
+            with lock:
+                while True:
+                    if errors or not pending:
+                        return None
+                    r = pending[0]
+                    b = state_bytes(r.spec)
+                    now = time.perf_counter() - t0
+                    fits = self.state_used + b <= self.state_budget or self.state_used == 0
+                    if r.arrival <= now and fits:
+                        break
+                    lock.wait(timeout=max(1e-3, r.arrival - now) if fits else None)
+                pending.popleft()
+                r.t_admit = now
+                r.state_bytes = b
+                self.state_used += b
+                self.peak_state = max(self.peak_state, self.state_used)
+                return r
+
+        def worker():
+            ctx = None
+            try:
+                torch.cuda.set_device(device)
+                ctx = api.Context(device)
+                with torch.cuda.stream(torch.cuda.Stream()):
+                    while (r := next_request()) is not None:
+                        self._serve_fp64(r, ctx)
+                        with lock:
+                            self._finish(r, time.perf_counter() - t0)
+                            lock.notify_all()
+            except BaseException as e:   # surfaced after the join
+                with lock:
+                    errors.append(e)
+                    lock.notify_all()
+            finally:
+                if ctx is not None:
+                    torch.cuda.synchronize(device)
+                    ctx.close()
+
+        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.concurrency)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
 
 
 def summarize(requests: list[Request]) -> dict:
