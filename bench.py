@@ -349,8 +349,8 @@ def run_ours(a, rank, world, local_rank):
     out["ms_per_timestep"] = {k: round(sum(getattr(r["times"], k) for r in recs) / len(recs), 3)
                               for k in ("deposit_ms", "solve_ms", "advect_ms", "rebin_ms")}
     achieved = bytes_local / (loop_ms * 1e-3) / 1e9
-    # DRAM bytes (read + write) of one k_pt_iter launch from the ncu capture in
-    # profiles/k_pt_iter_plume2048.md (2047^2 points), scaled by the point count
+    # DRAM bytes (read + write) of one k_pt_iter launch, measured by ncu at 2047^2 points, scaled by the
+    # point count (the kernel streams each field once, so its traffic grows with the points)
     traffic = TRAFFIC_PER_LAUNCH_2048 * ((a.n - 1) / 2047.0) ** 2
     out["roofline"] = {"bound": "hbm", "kernel": "k_pt_iter (fused PT iteration)", "achieved": round(achieved, 1),
                        "peak": peak, "peak_source": peak_src, "unit": "GB/s", "frac": round(achieved / peak, 4),

@@ -103,8 +103,11 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
  * SF_NOALLOC_MAX_MARKERS markers and grids with (nx+1)*(ny+1) <=
  * SF_NOALLOC_MAX_CELLS, and returns SF_ERR_TOO_LARGE beyond that.  It runs on
  * the calling thread's current device.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) and caches it; make that
- * first call before any stream capture.  All calls share the one array, so
+ * the array's device address (cudaGetSymbolAddress) and the device's SM count
+ * and caches both for the life of the process; make that first call before
+ * any stream capture.  A cudaDeviceReset (or any teardown of the device's
+ * primary context) invalidates that cache: after one, do not call this entry
+ * point again in the same process.  All calls share the one array, so
  * calls whose work overlaps on the GPU (different streams, or different host
  * threads on the same device) race and must be serialised by the caller.
  * Warning counts are not reported.  val_wt_sum / wt_sum are not produced. */

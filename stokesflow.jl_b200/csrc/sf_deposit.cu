@@ -279,26 +279,33 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
 constexpr int NA_MAX_DEVICES = 64;
 static unsigned char* g_noalloc_ptr[NA_MAX_DEVICES] = {};
+static int g_noalloc_sms[NA_MAX_DEVICES] = {};
 static std::mutex g_noalloc_mutex;
 
-// Device address of g_noalloc_scratch on the current device.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device (with that device current) and cached.
-static int noalloc_scratch(unsigned char** out) {
+// Device address of g_noalloc_scratch and the SM count of the current device.
+// In host code the array's name is only a host-side stand-in, so the address
+// is looked up once per device (with that device current) and cached, with
+// the SM count that sizes the marker kernels' grids.  A device reset
+// invalidates the cache (documented at the declaration).
+static int noalloc_scratch(unsigned char** out, int* num_sms) {
     int dev = 0;
     SF_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NA_MAX_DEVICES) return fail(SF_ERR_NO_DEVICE, "noalloc deposit: device index too large");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
+        int sms = 0;
+        SF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
             (void)cudaGetLastError();
             return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__);
         }
+        g_noalloc_sms[dev] = std::max(1, sms);
         g_noalloc_ptr[dev] = (unsigned char*)p;
     }
     *out = g_noalloc_ptr[dev];
+    *num_sms = g_noalloc_sms[dev];
     return SF_OK;
 }
 
@@ -319,7 +326,8 @@ extern "C" int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_gr
                                           std::to_string(ny) + " grid exceeds the fixed scratch (at most " +
                                           std::to_string(NA_MAX_CELLS) + " cells (nx+1)*(ny+1))");
     unsigned char* base = nullptr;
-    int rc = noalloc_scratch(&base);
+    int num_sms = 0;
+    int rc = noalloc_scratch(&base, &num_sms);
     if (rc) return rc;
     cudaStream_t s = as_stream(stream);
     int32_t* keys = (int32_t*)(base + NA_OFF_KEYS);
@@ -334,7 +342,9 @@ extern "C" int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_gr
     SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s));
-    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nm, DEP_THREADS), 148 * 32));
+    // grid-stride marker kernels: up to 32 blocks per SM of this device
+    const unsigned blocks =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nm, DEP_THREADS), (int64_t)num_sms * 32));
     if (nm > 0) {
         k_cell_keys<<<blocks, DEP_THREADS, 0, s>>>(x_m, y_m, nm, x_grid_min, y_grid_min, dx, dy, nx, ny, keys, counts,
                                                    counters + 0);

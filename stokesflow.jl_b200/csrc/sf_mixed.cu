@@ -870,6 +870,7 @@ struct Slot {  // an admitted instance
     bool swept = false;        // ran sweeps since its last fold
     int budget = 0;            // sweeps of its last round
     int64_t ncheck = 0, ndtupdate = 0;   // the reference's event periods for this grid (:35-36)
+    int64_t base = 0;          // inner_total when the current attempt started (a retry starts a new schedule)
     int64_t inner_total = 0, outer = 0;
     double err = 0.0, eps = 0.0;   // err of the last residual check (2 eps before the first, as :40)
     std::chrono::steady_clock::time_point t_submit;
@@ -1527,6 +1528,7 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
             const int64_t done = h.inner_total, outer = h.outer;
             if ((rc = admit(e, q, *h.user, 1))) return rc;
             h.inner_total = done;
+            h.base = done;
             h.outer = outer;
             h.err = 2.0 * h.eps;
             h.user->retried = 1;
@@ -1550,16 +1552,17 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
         SF_CUDA(cudaStreamWaitEvent(caller, e->ev_out, 0));
     }
     if (sweep.empty()) return SF_OK;
-    // budgets: up to the next event of each instance (relative iteration counts; a restarted instance keeps
-    // counting), at most fold_every
+    // budgets: up to the next event of each instance, at most fold_every.  Events are counted from the start
+    // of the current attempt (a restarted instance runs the schedule of a fresh solve); max_sweeps counts the
+    // sweeps of every attempt.
     for (int q : sweep) {
         Slot& h = e->slots[q];
         Ctl& c = e->h_ctl[q];
-        const int64_t it = h.inner_total;
+        const int64_t it = h.inner_total - h.base;
         int64_t b = std::min<int64_t>(K, h.ncheck - it % h.ncheck);
         const bool stab = h.d.use_stab != 0;
         if (stab) b = std::min<int64_t>(b, h.ndtupdate - it % h.ndtupdate);
-        b = std::max<int64_t>(1, std::min<int64_t>(b, max_sweeps - it));
+        b = std::max<int64_t>(1, std::min<int64_t>(b, max_sweeps - h.inner_total));
         const int64_t end = it + b;
         c.budget = (int)b;
         c.flags = ((end % h.ncheck == 0) ? CTL_CHECK : 0) | ((stab && end % h.ndtupdate == 0) ? CTL_DT : 0);

@@ -127,6 +127,22 @@ def _ctx(ctx: Context | None) -> Context:
     return ctx if ctx is not None else default_context()
 
 
+def _one_device(*tensors) -> torch.device:
+    """The CUDA device all the given tensors (None skipped) live on; ValueError if they are on several."""
+    devs = {t.device for t in tensors if t is not None}
+    if len(devs) != 1:
+        raise ValueError(f"the arrays must be on one CUDA device, got {sorted(str(d) for d in devs)}")
+    return devs.pop()
+
+
+def _ctx_on(ctx: Context | None, device: torch.device) -> Context:
+    """ctx (or the default context of `device`), checked to run on the device the arrays are on."""
+    c = ctx if ctx is not None else default_context(device.index)
+    if c.device != device.index:
+        raise ValueError(f"the context runs on cuda:{c.device}, the arrays are on {device}")
+    return c
+
+
 # ---------------------------------------------------------------------------
 def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, dx, dy, val_wt_sum=None,
                             wt_sum=None, grid=None, *, ctx: Context | None = None, stream=None):
@@ -145,9 +161,11 @@ def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, d
         ps = _grid(val_wt_sum, "val_wt_sum")
         pw = _grid(wt_sum, "wt_sum", val_wt_sum.shape)
         ld, n_sum = wt_sum.shape[0], wt_sum.numel()
-    c = _ctx(ctx)
+    dev = _one_device(val_grid, x_m, y_m, val_m, val_wt_sum, wt_sum)
+    c = _ctx_on(ctx, dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
     check(lib().sf_bilinear_marker_to_grid(c.handle, float(x_grid_min), float(y_grid_min), pg, nx, ny, px, py, pv,
-                                           nm, float(dx), float(dy), ps, pw, ld, n_sum, _stream(stream)),
+                                           nm, float(dx), float(dy), ps, pw, ld, n_sum, _stream(st)),
           "bilinear_marker_to_grid")
 
 
@@ -157,15 +175,19 @@ def bilinear_marker_to_grid_noalloc(x_grid_min, y_grid_min, val_grid, x_m, y_m, 
     stream loop that cudaMalloc's device-wide synchronisation would stall, a fixed memory budget).
     Scratch is a fixed array inside the library, so at most SF_NOALLOC_MAX_MARKERS markers and
     (nx+1)*(ny+1) <= SF_NOALLOC_MAX_CELLS; calls that overlap on the GPU race (they share that array).
-    Runs on the current device; no context is used."""
+    Runs on the device the arrays are on (all four must share it), on that device's current stream unless
+    `stream` is given; no context is used."""
     nx, ny = val_grid.shape
     nm = x_m.numel()
     if y_m.numel() != nm or val_m.numel() != nm:
         raise ValueError("x_m, y_m, val_m must have the same length")
-    check(lib().sf_bilinear_marker_to_grid_noalloc(float(x_grid_min), float(y_grid_min), _grid(val_grid, "val_grid"),
-                                                   nx, ny, _vec(x_m, "x_m"), _vec(y_m, "y_m"), _vec(val_m, "val_m"),
-                                                   nm, float(dx), float(dy), _stream(stream)),
-          "bilinear_marker_to_grid_noalloc")
+    dev = _one_device(val_grid, x_m, y_m, val_m)
+    pg, px, py, pv = _grid(val_grid, "val_grid"), _vec(x_m, "x_m"), _vec(y_m, "y_m"), _vec(val_m, "val_m")
+    with torch.cuda.device(dev):
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        check(lib().sf_bilinear_marker_to_grid_noalloc(float(x_grid_min), float(y_grid_min), pg, nx, ny, px, py, pv,
+                                                       nm, float(dx), float(dy), _stream(st)),
+              "bilinear_marker_to_grid_noalloc")
 
 
 def solve_stokes_info(P, Vx_pad, Vy_pad, rho_vy, mu_b, mu_p, txx, tyy, txy, divV, dtPt, Rx, Ry, dVxdt, dVydt, dtVx,

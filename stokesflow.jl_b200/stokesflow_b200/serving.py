@@ -65,11 +65,13 @@ def poisson_requests(n: int, rate: float, seed: int = 0, *, cells=(63, 2047), ti
                      mu_log10=(-2.0, 1.0), mu_air=1e-2) -> list[Request]:
     """n requests with exponential inter-arrival times of mean 1/rate seconds; cells per side log-uniform
     in `cells` (square grids), timesteps uniform in `timesteps`, materials as workloads.batch_specs."""
-    rng = np.random.default_rng(seed)
+    # arrivals and request contents from two streams of the seed, so that one does not shift the other
+    rng_t = np.random.default_rng([seed, 0])
+    rng = np.random.default_rng([seed, 1])
     t = 0.0
     out = []
     for k in range(n):
-        t += float(rng.exponential(1.0 / rate)) if rate > 0 else 0.0
+        t += float(rng_t.exponential(1.0 / rate)) if rate > 0 else 0.0
         c = log_uniform_int(rng, *cells)
         m = int(rng.integers(md[0], md[1] + 1))
         model = random_inclusion_model(rng, mu_log10=mu_log10, mu_air=mu_air)

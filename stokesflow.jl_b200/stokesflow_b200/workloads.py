@@ -64,18 +64,31 @@ def log_uniform_int(rng, lo, hi) -> int:
     return int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
 
 
+# gap of matrix kept between two inclusions, and draws of a position before an inclusion is left out
+INCLUSION_GAP = 0.03
+PLACEMENT_TRIES = 100
+
+
 def random_inclusion_model(rng, *, n_inclusions=(1, 3), radius=(0.05, 0.2), rho=(0.8, 1.2), mu_log10=(-2.0, 1.0),
                            air_height=0.1, rho_air=1e-3, mu_air=1e-2) -> InclusionModel:
+    """1-3 circular inclusions in a matrix of mu = 1, each touching only the matrix: it stays clear of the
+    air layer and of the other inclusions by a gap of matrix.  The reference's PT scheme converges for a
+    body of 1e-2 to 20 times the matrix viscosity against the matrix alone; a stiff body against the air
+    (1e3) or against a soft body (1e-2 next to 10 is a 1e3 jump) makes it diverge (tests/
+    test_oracle_contrast.py)."""
     k = int(rng.integers(n_inclusions[0], n_inclusions[1] + 1))
     inc = []
     for _ in range(k):
         r = float(rng.uniform(*radius))
-        cx = float(rng.uniform(0.2, 0.8))
-        # the inclusion stays clear of the air layer: a stiff inclusion against the air makes a 1e3 viscosity
-        # jump, where the reference's PT scheme diverges
+        rh = float(rng.uniform(*rho))
+        mu = float(10.0 ** rng.uniform(*mu_log10))
         top = air_height + r + 0.05
-        cy = float(rng.uniform(top, max(top, 0.95 - r)))
-        inc.append((cx, cy, r, float(rng.uniform(*rho)), float(10.0 ** rng.uniform(*mu_log10))))
+        for _ in range(PLACEMENT_TRIES):
+            cx = float(rng.uniform(0.2, 0.8))
+            cy = float(rng.uniform(top, max(top, 0.95 - r)))
+            if all((cx - x) ** 2 + (cy - y) ** 2 >= (r + q + INCLUSION_GAP) ** 2 for (x, y, q, _, _) in inc):
+                inc.append((cx, cy, r, rh, mu))
+                break
     return InclusionModel(air_height=air_height, rho_air=rho_air, mu_air=mu_air, inclusions=inc)
 
 

@@ -8,7 +8,7 @@ from, so the tests can pin the oracle without the reference present:
 * test/test_StokesFlow2D.jl:86-88   5 timesteps of the full loop, Vx / Vy at 10 indices
 * test/test_MarkerToGrid.jl:24-37   hand-computed 3x2 deposit
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py <StokesFlow.jl checkout>   (or set STOKESFLOW_REFERENCE)
 """
 from __future__ import annotations
 
@@ -62,4 +62,8 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: first argument, else $STOKESFLOW_REFERENCE
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("STOKESFLOW_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <StokesFlow.jl checkout>  (or set STOKESFLOW_REFERENCE)")
+    main(ref)

@@ -17,9 +17,14 @@ def test_batch_specs_are_seeded_and_in_range():
     for s in a:
         assert 128 <= s.Nx <= 1024 and 128 <= s.Ny <= 1024 and 3 <= s.md <= 5
         assert 1 <= len(s.model.inclusions) <= 3
-        for (cx, cy, r, rho, mu) in s.model.inclusions:
+        inc = s.model.inclusions
+        for (cx, cy, r, rho, mu) in inc:
             assert 0.05 <= r <= 0.2 and 0.8 <= rho <= 1.2 and 1e-2 <= mu <= 1e1
             assert cy - r >= 0.1 + 0.05 - 1e-12  # clear of the air layer
+        for i in range(len(inc)):                 # and of each other, by a gap of matrix
+            for j in range(i):
+                d = math.hypot(inc[i][0] - inc[j][0], inc[i][1] - inc[j][1])
+                assert d >= inc[i][2] + inc[j][2] + workloads.INCLUSION_GAP - 1e-12
 
 
 def test_log_uniform_sizes_cover_the_range():

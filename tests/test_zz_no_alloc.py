@@ -8,6 +8,10 @@ the library that every call shares, so these tests call it twice in a row
 (and once more with the first inputs) and check each result against the
 regular entry point, sf_bilinear_marker_to_grid, bit for bit -- the tolerance
 every deposit test here uses.  Both entry points are called through the C ABI.
+One case is also checked directly against the CPU oracle's serial deposit, and
+one test checks the property the entry point exists for: a call, after the
+first on the device, leaves the device's free memory and the context's scratch
+exactly as they were.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test; it also passes on its own in a fresh process.
@@ -86,3 +90,39 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(sf):
     rc = L.sf_bilinear_marker_to_grid_noalloc(0.0, 0.0, g.data_ptr(), 600, 600, t.data_ptr(), t.data_ptr(),
                                               t.data_ptr(), 4, 1.0, 1.0, None)
     assert rc == sf._lib.SF_ERR_TOO_LARGE
+
+
+def test_noalloc_matches_the_oracle(sf, oracle_lib):
+    """The first case against the oracle's serial deposit (MarkerToGrid.jl:110-172 restated in C): the
+    same bits, erroneous markers skipped and empty nodes keeping their value in both."""
+    seed, nx, ny, nm, dx, dy, x0, y0 = CASES[0]
+    x, y, v, start = _case(seed, nx, ny, nm, dx, dy, x0, y0)
+    xt, yt, vt = (torch.from_numpy(a).cuda() for a in (x, y, v))
+    g = _col(start)
+    _call_noalloc(sf, x0, y0, g, xt, yt, vt, dx, dy)
+    ref = np.asfortranarray(start.copy())
+    vws, ws = oracle_lib.zeros(nx, ny), oracle_lib.zeros(nx, ny)
+    oracle_lib.bilinear_marker_to_grid(x0, y0, ref, x, y, v, dx, dy, vws, ws)
+    assert np.array_equal(g.cpu().numpy(), ref)
+
+
+def test_noalloc_allocates_nothing(sf):
+    """After a first call (which looks up the scratch address and loads the kernels), further calls on new
+    grid sizes and marker counts change neither the device's free memory nor the default context's
+    scratch."""
+    seed, nx, ny, nm, dx, dy, x0, y0 = CASES[1]
+    x, y, v, start = _case(seed, nx, ny, nm, dx, dy, x0, y0)
+    xt, yt, vt = (torch.from_numpy(a).cuda() for a in (x, y, v))
+    g = _col(start)
+    _call_noalloc(sf, x0, y0, g, xt, yt, vt, dx, dy)
+    small = _col(np.zeros((40, 30)))
+    torch.cuda.synchronize()
+    scratch0 = sf.default_context().scratch_bytes()
+    free0, _ = torch.cuda.mem_get_info()
+    for grid, k in ((small, nm // 3), (g, nm)):
+        _call_noalloc(sf, x0, y0, grid, xt[:k], yt[:k], vt[:k], 0.025 if grid is small else dx,
+                      0.035 if grid is small else dy)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+    assert sf.default_context().scratch_bytes() == scratch0
