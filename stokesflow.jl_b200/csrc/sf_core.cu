@@ -321,7 +321,7 @@ int sf_ctx_destroy(sf_ctx* c) {
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();
     mixed_engine_release(c);
-    Scratch* all[] = {&c->keys,     &c->counts, &c->offsets,  &c->cursor, &c->perm,
+    Scratch* all[] = {&c->keys,     &c->counts, &c->offsets,  &c->cursor, &c->perm,  &c->payload, &c->longs,
                       &c->scan_tmp, &c->fields, &c->partials, &c->mixed,  &c->exch};
     for (Scratch* s : all)
         if (s->ptr) cudaFree(s->ptr);
@@ -339,7 +339,7 @@ int sf_ctx_destroy(sf_ctx* c) {
 
 int sf_ctx_scratch_bytes(sf_ctx* c, int64_t* bytes) {
     if (!c || !bytes) return fail(SF_ERR_INVALID_ARG, "sf_ctx_scratch_bytes: NULL argument");
-    const Scratch* all[] = {&c->keys,     &c->counts, &c->offsets,  &c->cursor, &c->perm,
+    const Scratch* all[] = {&c->keys,     &c->counts, &c->offsets,  &c->cursor, &c->perm,  &c->payload, &c->longs,
                             &c->scan_tmp, &c->fields, &c->partials, &c->mixed,  &c->exch};
     int64_t b = 0;
     for (const Scratch* s : all) b += (int64_t)s->bytes;

@@ -8,15 +8,27 @@
 //                      topleftIndexRelDist (common.jl:22-33); per-cell counts
 //                      with warp-aggregated integer atomics.
 //   2. exclusive scan  counts -> cell offsets.
-//   3. k_scatter       marker indices into their cell's segment.
-//   4. k_sort_segments each segment sorted ascending (insertion sort; a cell
-//                      holds ~16-25 markers), giving a stable counting sort.
-//   5. k_gather        one thread per node merges the four adjacent cells'
+//   3. k_scatter       marker indices into their cell's segment (in no
+//                      particular order inside it).
+//   4. segment sort    every segment ascending by marker index, which makes
+//                      the whole a stable counting sort:
+//                      k_long_cells + k_sort_long sort the cells holding more
+//                      than SORT_LONG markers in place (a block-wide LSD radix
+//                      sort per cell, stable, linear in the cell's count, so a
+//                      cell where markers pile up costs no more than its
+//                      size); k_sort_cells sorts the others in shared memory,
+//                      a window of consecutive cells at a time.
+//   5. k_gather_sorted one thread per node merges the four adjacent cells'
 //                      segments by marker index and accumulates w and w*val in
 //                      ascending marker order -- the reference CPU loop's
 //                      order, so each node's sums are bit-identical to it --
 //                      then divides (safeDivision, :164-172).
-// Steps 1-4 are also the rebin (sf_rebin_markers).
+// For the deposit, step 4 writes each sorted entry as a payload record
+// {dxij, dyij, val, m} (the marker's relative position in its cell, computed
+// once with topleftIndexRelDist's IEEE divisions, its value and its index), so
+// the gather streams contiguous records of neighbouring cells instead of
+// chasing marker indices into x, y and val.  Steps 1-4 with the permutation as
+// output are the rebin (sf_rebin_markers).
 #include <algorithm>
 
 #include "sf_internal.cuh"
@@ -24,6 +36,17 @@
 namespace sf {
 
 constexpr int DEP_THREADS = 256;
+constexpr int SORT_THREADS = 256;
+constexpr int SORT_CPB = 256;     // cells per block of k_sort_cells
+constexpr int SORT_CAP = 4096;    // entries of a k_sort_cells window in shared memory
+constexpr int SORT_LONG = 64;     // cells with more markers are sorted by k_sort_long
+
+// A sorted deposit entry: the marker's relative position in its cell (topleftIndexRelDist's dxij, dyij), its
+// value and its index.  32 bytes: one sector.
+struct __align__(32) Payload {
+    double dxij, dyij, val;
+    int32_t m, pad_;
+};
 
 // 1. cell key of every marker; counts[key]++ (warp-aggregated).
 __global__ void k_cell_keys(const double* __restrict__ x, const double* __restrict__ y, int64_t nm, double xmin,
@@ -77,11 +100,13 @@ __global__ void k_scatter(const int32_t* __restrict__ keys, int64_t nm, const in
     }
 }
 
-// 4. sort every cell segment ascending (one thread per cell).
+// The allocation-free deposit's per-cell sort of short segments (one thread per cell; its long segments are
+// sorted by k_sort_long first, and are skipped here).
 __global__ void k_sort_segments(const int32_t* __restrict__ offsets, int64_t ncells, int32_t* __restrict__ perm) {
     int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= ncells) return;
     int32_t b = offsets[c], e = offsets[c + 1];
+    if (e - b > SORT_LONG) return;
     for (int32_t i = b + 1; i < e; ++i) {
         int32_t v = perm[i];
         int32_t j = i - 1;
@@ -94,6 +119,221 @@ __global__ void k_sort_segments(const int32_t* __restrict__ offsets, int64_t nce
     }
 }
 
+// 4a. the cells holding more than SORT_LONG markers -> list[0 .. *n_list)
+__global__ void k_long_cells(const int32_t* __restrict__ offsets, int64_t ncells, int32_t* __restrict__ list,
+                             int32_t* __restrict__ n_list) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncells; c += (int64_t)gridDim.x * blockDim.x)
+        if (offsets[c + 1] - offsets[c] > SORT_LONG) list[atomicAdd(n_list, 1)] = (int32_t)c;
+}
+
+// 4b. each long cell's segment sorted ascending in place by a block-wide LSD radix sort on 8-bit digits of the
+// marker index (indices are non-negative 31-bit values: 4 digits), stable, through `tmp` at the same offsets.
+// A digit on which the whole segment agrees moves nothing and is skipped.  Tiles of SORT_THREADS entries are
+// ranked in order: lanes within a warp by __match_any_sync, warps by their per-digit counts.
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_long(const int32_t* __restrict__ offsets,
+                                                            const int32_t* __restrict__ list,
+                                                            const int32_t* __restrict__ n_list, int32_t* perm,
+                                                            int32_t* tmp) {
+    constexpr int NW = SORT_THREADS / 32;
+    __shared__ int hist[256];
+    __shared__ int base[256];
+    __shared__ int wcnt[NW][256];
+    __shared__ int skip;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int n_long = *n_list;
+    for (int li = blockIdx.x; li < n_long; li += gridDim.x) {
+        const int c = list[li];
+        const int32_t b = offsets[c], n = offsets[c + 1] - b;
+        int32_t* src = perm + b;
+        int32_t* dst = tmp + b;
+        for (int shift = 0; shift < 32; shift += 8) {
+            hist[tid] = 0;
+            __syncthreads();
+            for (int i = tid; i < n; i += SORT_THREADS) atomicAdd(&hist[(src[i] >> shift) & 255], 1);
+            __syncthreads();
+            if (tid == 0) {
+                int run = 0, same = 0;
+                for (int d = 0; d < 256; ++d) {
+                    base[d] = run;
+                    run += hist[d];
+                    same |= (hist[d] == n);
+                }
+                skip = same;
+            }
+            __syncthreads();
+            if (skip) continue;
+            for (int t0 = 0; t0 < n; t0 += SORT_THREADS) {
+                for (int k = tid; k < NW * 256; k += SORT_THREADS) (&wcnt[0][0])[k] = 0;
+                __syncthreads();
+                const int i = t0 + tid;
+                const bool valid = i < n;
+                const int32_t v = valid ? src[i] : 0;
+                const int d = (v >> shift) & 255;
+                const unsigned act = __ballot_sync(0xffffffffu, valid);
+                int rank = 0;
+                if (valid) {
+                    const unsigned peers = __match_any_sync(act, d);
+                    rank = __popc(peers & ((1u << lane) - 1u));
+                    if (lane == __ffs(peers) - 1) wcnt[warp][d] = __popc(peers);
+                }
+                __syncthreads();
+                if (valid) {
+                    int off = base[d] + rank;
+                    for (int w = 0; w < warp; ++w) off += wcnt[w][d];
+                    dst[off] = v;
+                }
+                __syncthreads();
+                int sum = 0;
+                for (int w = 0; w < NW; ++w) sum += wcnt[w][tid];
+                base[tid] += sum;
+                __syncthreads();
+            }
+            int32_t* t = src;
+            src = dst;
+            dst = t;
+        }
+        if (src != perm + b)
+            for (int i = tid; i < n; i += SORT_THREADS) perm[b + i] = src[i];
+        __syncthreads();
+    }
+}
+
+// 4c. every short segment sorted ascending; long segments (sorted by k_sort_long) pass through in order.  A
+// block takes SORT_CPB consecutive cells and works through them in windows of consecutive cells holding at most
+// SORT_CAP entries: it loads a window's marker indices into shared memory, ranks each entry within its cell by
+// counting the smaller indices there, and writes it to its sorted place -- back into perm (the rebin), or as a
+// payload record (the deposit: topleftIndexRelDist of the marker and its value, once per marker).
+template <bool PAYLOAD>
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_cells(const int32_t* __restrict__ offsets, int64_t ncells,
+                                                             int32_t* perm, Payload* __restrict__ out,
+                                                             const double* __restrict__ x, const double* __restrict__ y,
+                                                             const double* __restrict__ val, double xmin, double ymin,
+                                                             double dx, double dy) {
+    __shared__ int32_t soff[SORT_CPB + 1];
+    __shared__ int32_t sm[SORT_CAP];
+    const int tid = threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.x * SORT_CPB;
+    if (c0 >= ncells) return;
+    const int nc = (int)min((int64_t)SORT_CPB, ncells - c0);
+    for (int i = tid; i <= nc; i += SORT_THREADS) soff[i] = offsets[c0 + i];
+    __syncthreads();
+    auto emit = [&](int32_t pos, int32_t m) {
+        if (PAYLOAD) {
+            const TopLeft t = topleft(xmin, ymin, x[m], y[m], dx, dy);
+            Payload p;
+            p.dxij = t.dxij;
+            p.dyij = t.dyij;
+            p.val = val[m];
+            p.m = m;
+            p.pad_ = 0;
+            out[pos] = p;
+        } else {
+            perm[pos] = m;
+        }
+    };
+    int w0 = 0;
+    while (w0 < nc) {
+        // the largest w1 with soff[w1] - soff[w0] <= SORT_CAP (w1 == w0: cell w0 alone holds more)
+        int lo = w0, hi = nc;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (soff[mid] - soff[w0] <= SORT_CAP) lo = mid; else hi = mid - 1;
+        }
+        const int w1 = lo;
+        if (w1 == w0) {  // a long cell, sorted already: pass it through
+            if (PAYLOAD)
+                for (int32_t pos = soff[w0] + tid; pos < soff[w0 + 1]; pos += SORT_THREADS) emit(pos, perm[pos]);
+            ++w0;
+            continue;
+        }
+        const int32_t e0 = soff[w0];
+        const int ne = soff[w1] - e0;
+        for (int i = tid; i < ne; i += SORT_THREADS) sm[i] = perm[e0 + i];
+        __syncthreads();
+        for (int i = tid; i < ne; i += SORT_THREADS) {
+            // the entry's cell k: the last one in [w0, w1) starting at or before it
+            int a = w0, z = w1 - 1;
+            while (a < z) {
+                const int mid = (a + z + 1) >> 1;
+                if (soff[mid] - e0 <= i) a = mid; else z = mid - 1;
+            }
+            const int cb = soff[a] - e0, ce = soff[a + 1] - e0;
+            int rank = i - cb;
+            if (ce - cb <= SORT_LONG) {
+                const int32_t v = sm[i];
+                rank = 0;
+                for (int j = cb; j < ce; ++j) rank += (sm[j] < v) ? 1 : 0;
+            }
+            emit(e0 + cb + rank, sm[i]);
+        }
+        __syncthreads();
+        w0 = w1;
+    }
+}
+
+// 5. per-node gather over the sorted payload.  Node (I, J), 1-based.  A marker in cell (ix, iy) contributes to
+// node (ix, iy) with (1-dx)(1-dy), (ix+1, iy) with dx(1-dy), (ix, iy+1) with (1-dx)dy and (ix+1, iy+1) with dx*dy
+// (MarkerToGrid.jl:124-151), so node (I, J) merges the cells (I,J), (I-1,J), (I,J-1), (I-1,J-1), whose records
+// are sorted by marker index: taking the smallest head each time visits the node's markers in ascending
+// index order, the reference's serial order.  The records of neighbouring cells are neighbours in memory, so
+// the threads of a warp (neighbouring nodes of a grid row) walk overlapping, contiguous runs of records.
+__global__ void __launch_bounds__(DEP_THREADS) k_gather_sorted(const Payload* __restrict__ pl,
+                                                               const int32_t* __restrict__ offsets, int64_t nx,
+                                                               int64_t ny, double* __restrict__ val_grid,
+                                                               double* __restrict__ val_wt_sum,
+                                                               double* __restrict__ wt_sum, int64_t ld_sum,
+                                                               unsigned long long* __restrict__ empty_counter) {
+    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (n >= nx * ny) return;
+    const int64_t I = n % nx + 1, J = n / nx + 1;
+    const int64_t ldc = nx + 1;
+    int32_t cur[4], end[4], head[4];
+    // corner k: 0 = marker's top-left node (cell I,J), 1 = top-right (cell I-1,J),
+    //           2 = bottom-left (cell I,J-1), 3 = bottom-right (cell I-1,J-1)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int64_t key = (I - (k & 1)) + (J - (k >> 1)) * ldc;
+        cur[k] = offsets[key];
+        end[k] = offsets[key + 1];
+        head[k] = (cur[k] < end[k]) ? pl[cur[k]].m : 0x7fffffff;
+    }
+    double ws = 0.0, vs = 0.0;
+    while (true) {
+        int kb = 0;
+        int32_t best = head[0];
+#pragma unroll
+        for (int k = 1; k < 4; ++k)
+            if (head[k] < best) {
+                best = head[k];
+                kb = k;
+            }
+        if (best == 0x7fffffff) break;
+        int32_t pos = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (k == kb) {
+                pos = cur[k]++;
+                head[k] = (cur[k] < end[k]) ? pl[cur[k]].m : 0x7fffffff;
+            }
+        const Payload p = pl[pos];
+        const double wx = (kb & 1) ? p.dxij : (1.0 - p.dxij);
+        const double wy = (kb >> 1) ? p.dyij : (1.0 - p.dyij);
+        const double w = wx * wy;
+        ws = ws + w;
+        vs = vs + w * p.val;
+    }
+    if (wt_sum) {
+        wt_sum[(I - 1) + (J - 1) * ld_sum] = ws;
+        val_wt_sum[(I - 1) + (J - 1) * ld_sum] = vs;
+    }
+    if (ws != 0.0)
+        val_grid[(I - 1) + (J - 1) * nx] = vs / ws;
+    else if (empty_counter)
+        atomicAdd(empty_counter, 1ull);
+}
+
+// The allocation-free deposit's gather (its scratch holds no payload): the same merge, reading each marker's
+// position and value through the sorted permutation.
 // 5. per-node gather.  Node (I, J), 1-based.  A marker in cell (ix, iy)
 // contributes to node (ix, iy) with (1-dx)(1-dy), (ix+1, iy) with dx(1-dy),
 // (ix, iy+1) with (1-dx)dy and (ix+1, iy+1) with dx*dy (MarkerToGrid.jl:124-151),
@@ -155,9 +395,10 @@ static unsigned grid_for(sf_ctx* ctx, int64_t n, int threads) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, threads), (int64_t)ctx->num_sms * 32));
 }
 
-// Steps 1-4: stable counting sort of markers by cell -> ctx->counts/offsets/perm.
-static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, int64_t nm, double xmin, double ymin,
-                        double dx, double dy, int64_t nx, int64_t ny, unsigned long long* bad_counter,
+// Steps 1-4: stable counting sort of markers by cell -> ctx->counts / offsets, and either the cell-ordered
+// permutation in ctx->perm or (with val) the cell-ordered payload records in ctx->payload.
+static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, const double* val, int64_t nm, double xmin,
+                        double ymin, double dx, double dy, int64_t nx, int64_t ny, unsigned long long* bad_counter,
                         cudaStream_t s) {
     int64_t ncells = (nx + 1) * (ny + 1);
     int rc;
@@ -166,13 +407,17 @@ static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, int64_t n
     if ((rc = ensure(ctx, ctx->counts, (size_t)(ncells + 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->offsets, (size_t)(ncells + 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->cursor, (size_t)(ncells + 1) * 4))) return rc;
+    if ((rc = ensure(ctx, ctx->longs, (size_t)(ncells + 1) * 4))) return rc;
+    if (val && (rc = ensure(ctx, ctx->payload, (size_t)std::max<int64_t>(nm, 1) * sizeof(Payload)))) return rc;
     int32_t* keys = (int32_t*)ctx->keys.ptr;
     int32_t* counts = (int32_t*)ctx->counts.ptr;
     int32_t* offsets = (int32_t*)ctx->offsets.ptr;
     int32_t* cursor = (int32_t*)ctx->cursor.ptr;
     int32_t* perm = (int32_t*)ctx->perm.ptr;
+    int32_t* n_long = (int32_t*)ctx->longs.ptr;   // the count, then the list
     SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(ncells + 1) * 4, s));
+    SF_CUDA(cudaMemsetAsync(n_long, 0, 4, s));
     if (nm > 0) {
         k_cell_keys<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(x, y, nm, xmin, ymin, dx, dy, nx, ny, keys,
                                                                              counts, bad_counter);
@@ -182,9 +427,20 @@ static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, int64_t n
     if (nm > 0) {
         k_scatter<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(keys, nm, offsets, cursor, perm);
         SF_LAUNCHED(ctx);
+        k_long_cells<<<grid_for(ctx, ncells, DEP_THREADS), DEP_THREADS, 0, s>>>(offsets, ncells, n_long + 1, n_long);
+        SF_LAUNCHED(ctx);
+        // the keys are spent: they are the radix sort's second buffer
+        k_sort_long<<<(unsigned)ctx->num_sms * 2, SORT_THREADS, 0, s>>>(offsets, n_long + 1, n_long, perm, keys);
+        SF_LAUNCHED(ctx);
+        const unsigned blocks = (unsigned)ceil_div(ncells, SORT_CPB);
+        if (val)
+            k_sort_cells<true><<<blocks, SORT_THREADS, 0, s>>>(offsets, ncells, perm, (Payload*)ctx->payload.ptr, x, y,
+                                                               val, xmin, ymin, dx, dy);
+        else
+            k_sort_cells<false><<<blocks, SORT_THREADS, 0, s>>>(offsets, ncells, perm, nullptr, x, y, val, xmin, ymin,
+                                                                dx, dy);
+        SF_LAUNCHED(ctx);
     }
-    k_sort_segments<<<(unsigned)ceil_div(ncells, 128), 128, 0, s>>>(offsets, ncells, perm);
-    SF_LAUNCHED(ctx);
     return SF_OK;
 }
 
@@ -209,17 +465,16 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
     int rc = set_device(ctx);
     if (rc) return rc;
     cudaStream_t s = as_stream(stream);
-    if ((rc = sort_by_cell(ctx, x_m, y_m, nm, x_grid_min, y_grid_min, dx, dy, nx, ny,
+    if ((rc = sort_by_cell(ctx, x_m, y_m, val_m, nm, x_grid_min, y_grid_min, dx, dy, nx, ny,
                            ctx->d_counters + CNT_BAD_MARKERS, s)))
         return rc;
     if (wt_sum) {
         SF_CUDA(cudaMemsetAsync(wt_sum, 0, (size_t)n_sum * 8, s));
         SF_CUDA(cudaMemsetAsync(val_wt_sum, 0, (size_t)n_sum * 8, s));
     }
-    int64_t nnodes = nx * ny;
-    k_gather<<<(unsigned)ceil_div(nnodes, DEP_THREADS), DEP_THREADS, 0, s>>>(
-        x_m, y_m, val_m, (const int32_t*)ctx->offsets.ptr, (const int32_t*)ctx->perm.ptr, nx, ny, x_grid_min,
-        y_grid_min, dx, dy, val_grid, val_wt_sum, wt_sum, ld_sum, ctx->d_counters + CNT_EMPTY_NODES);
+    k_gather_sorted<<<(unsigned)ceil_div(nx * ny, DEP_THREADS), DEP_THREADS, 0, s>>>(
+        (const Payload*)ctx->payload.ptr, (const int32_t*)ctx->offsets.ptr, nx, ny, val_grid, val_wt_sum, wt_sum,
+        ld_sum, ctx->d_counters + CNT_EMPTY_NODES);
     SF_LAUNCHED(ctx);
     return SF_OK;
 }
@@ -234,8 +489,8 @@ int sf_rebin_markers(sf_ctx* ctx, const double* x_m, const double* y_m, int64_t 
     int rc = set_device(ctx);
     if (rc) return rc;
     cudaStream_t s = as_stream(stream);
-    if ((rc = sort_by_cell(ctx, x_m, y_m, nm, x_grid_min, y_grid_min, dx, dy, nx, ny, ctx->d_counters + CNT_OUTSIDE,
-                           s)))
+    if ((rc = sort_by_cell(ctx, x_m, y_m, nullptr, nm, x_grid_min, y_grid_min, dx, dy, nx, ny,
+                           ctx->d_counters + CNT_OUTSIDE, s)))
         return rc;
     int64_t ncells = (nx + 1) * (ny + 1);
     if (counts) SF_CUDA(cudaMemcpyAsync(counts, ctx->counts.ptr, (size_t)ncells * 4, cudaMemcpyDeviceToDevice, s));
@@ -273,7 +528,7 @@ constexpr size_t NA_OFF_OFFSETS = NA_OFF_COUNTS + 4 * (NA_MAX_CELLS + 64);
 constexpr size_t NA_OFF_CURSOR = NA_OFF_OFFSETS + 4 * (NA_MAX_CELLS + 64);
 constexpr size_t NA_OFF_TILES = NA_OFF_CURSOR + 4 * (NA_MAX_CELLS + 64);
 constexpr size_t NA_OFF_COUNTERS = NA_OFF_TILES + 4 * ((NA_SCAN_TILES + 63) / 64 * 64);
-constexpr size_t NA_BYTES = NA_OFF_COUNTERS + 2 * sizeof(unsigned long long);
+constexpr size_t NA_BYTES = NA_OFF_COUNTERS + 4 * sizeof(unsigned long long);   // 2 counters, the long-cell count
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
@@ -338,10 +593,11 @@ extern "C" int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_gr
     int32_t* tiles = (int32_t*)(base + NA_OFF_TILES);
     unsigned long long* counters = (unsigned long long*)(base + NA_OFF_COUNTERS);
     const int64_t ncells = (nx + 1) * (ny + 1);
+    int32_t* n_long = (int32_t*)(counters + 2);
     // the array keeps the previous call's contents: clear what must start at zero
     SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(ncells + 1) * 4, s));
-    SF_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), s));
+    SF_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), s));
     // grid-stride marker kernels: up to 32 blocks per SM of this device
     const unsigned blocks =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nm, DEP_THREADS), (int64_t)num_sms * 32));
@@ -353,6 +609,12 @@ extern "C" int sf_bilinear_marker_to_grid_noalloc(double x_grid_min, double y_gr
     if ((rc = exclusive_scan_i32_into(counts, offsets, ncells, offsets + ncells, tiles, s))) return rc;
     if (nm > 0) {
         k_scatter<<<blocks, DEP_THREADS, 0, s>>>(keys, nm, offsets, cursor, perm);
+        SF_CHECK_LAUNCH();
+        // long segments by the radix sort (the spent cursors hold their list, the spent keys are its buffer),
+        // the others one thread per cell
+        k_long_cells<<<blocks, DEP_THREADS, 0, s>>>(offsets, ncells, cursor, n_long);
+        SF_CHECK_LAUNCH();
+        k_sort_long<<<(unsigned)num_sms * 2, SORT_THREADS, 0, s>>>(offsets, cursor, n_long, perm, keys);
         SF_CHECK_LAUNCH();
     }
     k_sort_segments<<<(unsigned)ceil_div(ncells, 128), 128, 0, s>>>(offsets, ncells, perm);

@@ -65,8 +65,9 @@ enum { SC_DT = 0, SC_DT_CHECK = 1, SC_ERR = 2, SC_SUM_RX = 3, SC_SUM_RY = 4, SC_
 struct sf_ctx {
     int device = 0;
     int num_sms = 148;
-    // deposit / rebin scratch
-    sf::Scratch keys, counts, offsets, cursor, perm, scan_tmp;
+    // deposit / rebin scratch: cell keys, counts, offsets, scatter cursors, the cell-ordered permutation, scan
+    // tiles, the deposit's sorted payload records and the list of long cells
+    sf::Scratch keys, counts, offsets, cursor, perm, scan_tmp, payload, longs;
     // PT solve: padded internal fields, reduction partials; mixed/batched engine arena
     sf::Scratch fields, partials, mixed;
     // decomposed timestep: marker-exchange and overlap-sum staging

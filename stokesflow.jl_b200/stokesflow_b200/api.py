@@ -396,15 +396,24 @@ def move_markers_rk4(x_m, y_m, Vx, Vy, x_vx_min, y_vx_min, x_vy_min, y_vy_min, d
                                     float(ly), float(dx), float(dy), _stream(stream)), "move_markers_rk4")
 
 
-def rebin_markers(x_m, y_m, x_grid_min, y_grid_min, dx, dy, nx, ny, *, ctx: Context | None = None, stream=None):
+def rebin_markers(x_m, y_m, x_grid_min, y_grid_min, dx, dy, nx, ny, *, out=None, ctx: Context | None = None,
+                  stream=None):
     """Stable counting sort of the markers by cell of an (nx, ny)-node grid.
-    Returns int32 CUDA tensors (counts[(nx+1)*(ny+1)], offsets[+1], perm[nm])."""
+    Returns int32 CUDA tensors (counts[(nx+1)*(ny+1)], offsets[+1], perm[nm]); `out` may give those three
+    tensors (sizes as above, perm at least max(nm, 1)) to be filled instead of new ones."""
     nm = x_m.numel()
     ncells = (nx + 1) * (ny + 1)
     dev = x_m.device
-    counts = torch.empty(ncells, dtype=torch.int32, device=dev)
-    offsets = torch.empty(ncells + 1, dtype=torch.int32, device=dev)
-    perm = torch.empty(max(nm, 1), dtype=torch.int32, device=dev)
+    if out is not None:
+        counts, offsets, perm = out
+        ok = all(t.dtype == torch.int32 and t.device == dev and t.is_contiguous() for t in out)
+        if not ok or counts.numel() != ncells or offsets.numel() != ncells + 1 or perm.numel() < max(nm, 1):
+            raise ValueError("rebin_markers: out must be int32 tensors on the markers' device of sizes "
+                             f"{ncells}, {ncells + 1} and >= {max(nm, 1)}")
+    else:
+        counts = torch.empty(ncells, dtype=torch.int32, device=dev)
+        offsets = torch.empty(ncells + 1, dtype=torch.int32, device=dev)
+        perm = torch.empty(max(nm, 1), dtype=torch.int32, device=dev)
     c = _ctx(ctx)
     check(lib().sf_rebin_markers(c.handle, _vec(x_m, "x_m"), _vec(y_m, "y_m"), nm, float(x_grid_min),
                                  float(y_grid_min), float(dx), float(dy), int(nx), int(ny), counts.data_ptr(),

@@ -127,6 +127,7 @@ class StokesFlow2D:
         self.t_tot = 0.0
         self.nt = 0
         self.counts = None
+        self._rebin_out = None
         self._ev = [torch.cuda.Event(enable_timing=True) for _ in range(8)]
         self.snapshots = None
         if self.snapshot_dir:   # StokesFlow2D_multixpu.jl:136-141: stats, markers and grid before the first step
@@ -181,8 +182,16 @@ class StokesFlow2D:
                              self.dt, self.lx, self.ly, self.dx, self.dy, ctx=self.ctx)
 
     def do_rebin(self):
-        self.counts, _, _ = api.rebin_markers(self.x_m, self.y_m, self.o["x"], self.o["y"], self.dx, self.dy,
-                                              self.Nx, self.Ny, ctx=self.ctx)
+        # the outputs are allocated once and filled in every timestep
+        nm, ncells = self.n_markers, (self.Nx + 1) * (self.Ny + 1)
+        if self._rebin_out is None or self._rebin_out[2].numel() < max(nm, 1):
+            dev = self.x_m.device
+            self._rebin_out = (torch.empty(ncells, dtype=torch.int32, device=dev),
+                               torch.empty(ncells + 1, dtype=torch.int32, device=dev),
+                               torch.empty(max(nm, 1), dtype=torch.int32, device=dev))
+        self.counts, self.cell_offsets, self.cell_perm = api.rebin_markers(
+            self.x_m, self.y_m, self.o["x"], self.o["y"], self.dx, self.dy, self.Nx, self.Ny, out=self._rebin_out,
+            ctx=self.ctx)
 
     def step(self, host_io: bool = False) -> dict:
         """One timestep.  host_io: the reference's per-timestep host round trip

@@ -101,6 +101,39 @@ def test_deposit_clustered_markers(sf, oracle_lib):
     assert np.array_equal(host(got), ref)
 
 
+def test_deposit_and_rebin_with_markers_piled_in_one_cell(sf, oracle_lib):
+    """Markers piled into single cells, as markers clamped into a corner pile up: one cell holds 10^5 markers
+    (more than a shared-memory window of the segment sort), another 2000, the rest of the grid ~25 per cell,
+    all indices shuffled.  The deposit (regular and allocation-free) equals the oracle's serial loop bit for
+    bit, and the rebin's permutation is sorted inside every cell."""
+    O = oracle_lib
+    nx, ny, dx, dy = 40, 30, 0.025, 0.03
+    rng = np.random.default_rng(12)
+    n0, n1, n2 = 30_000, 100_000, 2_000
+    x = np.concatenate([rng.random(n0) * (nx - 1) * dx, (5 + rng.random(n1)) * dx, (30 + rng.random(n2)) * dx])
+    y = np.concatenate([rng.random(n0) * (ny - 1) * dy, (7 + rng.random(n1)) * dy, (20 + rng.random(n2)) * dy])
+    order = rng.permutation(x.size)
+    x, y = x[order], y[order]
+    v = np.exp(rng.normal(size=x.size))
+    ref = F(nx, ny)
+    O.bilinear_marker_to_grid(0.0, 0.0, ref, x, y, v, dx, dy, F(nx, ny), F(nx, ny))
+    got = sf.zeros(nx, ny)
+    xt, yt, vt = dev(x), dev(y), dev(v)
+    sf.bilinear_marker_to_grid(0.0, 0.0, got, xt, yt, vt, dx, dy)
+    assert np.array_equal(host(got), ref)
+    na = sf.zeros(nx, ny)
+    sf.bilinear_marker_to_grid_noalloc(0.0, 0.0, na, xt, yt, vt, dx, dy)
+    assert np.array_equal(host(na), ref)
+    counts_o, _ = O.cell_counts(x, y, 0.0, 0.0, dx, dy, nx, ny)
+    counts, offsets, perm = sf.rebin_markers(xt, yt, 0.0, 0.0, dx, dy, nx, ny)
+    assert np.array_equal(counts.cpu().numpy(), counts_o) and counts_o.max() >= n1
+    off = offsets.cpu().numpy()
+    p = perm.cpu().numpy()[: off[-1]]
+    assert np.array_equal(np.sort(p), np.arange(x.size))
+    for c in range(counts_o.size):
+        assert np.all(np.diff(p[off[c]:off[c + 1]]) > 0), f"cell {c} not in marker order"
+
+
 # ---------------------------------------------------------------------------
 # solver
 # ---------------------------------------------------------------------------
@@ -182,6 +215,61 @@ def _shapes(Nx, Ny):
 # ---------------------------------------------------------------------------
 # advection + rebin
 # ---------------------------------------------------------------------------
+def _grid_line_markers(rng, xmins, ymins, dx, dy, kx, ky, n_rand):
+    """Markers on the grid lines of every given origin (x = xmin + k dx exactly, as the reference computes the
+    node coordinate) and one and two ulps to either side, plus random ones: the positions where
+    floor((x - xmin)/dx) and (x - x_ix)/dx sit on their boundaries."""
+    xs, ys = [], []
+    for x0, y0 in zip(xmins, ymins):
+        for k in range(kx):
+            base = x0 + k * dx
+            for v in (base, np.nextafter(base, -np.inf), np.nextafter(base, np.inf),
+                      np.nextafter(np.nextafter(base, -np.inf), -np.inf), np.nextafter(np.nextafter(base, np.inf), np.inf)):
+                xs.append(v)
+                ys.append(y0 + rng.integers(0, ky) * dy + rng.random() * dy)
+        for k in range(ky):
+            base = y0 + k * dy
+            for v in (base, np.nextafter(base, -np.inf), np.nextafter(base, np.inf)):
+                ys.append(v)
+                xs.append(x0 + rng.integers(0, kx) * dx + rng.random() * dx)
+    x = np.concatenate([np.array(xs), rng.random(n_rand) * (kx - 1) * dx])
+    y = np.concatenate([np.array(ys), rng.random(n_rand) * (ky - 1) * dy])
+    return x, y
+
+
+def test_divisions_on_grid_lines_bitexact(sf, oracle_lib):
+    """topleftIndexRelDist's divisions run as a reciprocal multiply with a proved correctly rounded result
+    (the IEEE division where the proof fails): on markers sitting on the grid lines of all three deposit grids
+    and of the velocity grids, and 1-2 ulps off them, the deposits and the RK4 advection stay bit-identical to
+    the oracle's IEEE divisions."""
+    O = oracle_lib
+    Nx, Ny = 33, 27
+    dx, dy = 1.0 / (Nx - 1), 0.9 / (Ny - 1)
+    lx, ly = (Nx - 1) * dx, (Ny - 1) * dy
+    o = O.node_origins(dx, dy)
+    rng = np.random.default_rng(21)
+    x, y = _grid_line_markers(rng, [o["x"], o["x_p"], o["x_rho"], o["x_vx"], o["x_vy"]],
+                              [o["y"], o["y_p"], o["y_rho"], o["y_vx"], o["y_vy"]], dx, dy, Nx, Ny, 20000)
+    x = np.clip(x, 0.0, lx)
+    y = np.clip(y, 0.0, ly)
+    v = np.exp(rng.normal(size=x.size))
+    for x0, y0, shape in ((o["x_rho"], o["y_rho"], (Nx + 1, Ny)), (o["x"], o["y"], (Nx, Ny)),
+                          (o["x_p"], o["y_p"], (Nx - 1, Ny - 1))):
+        ref = F(*shape)
+        O.bilinear_marker_to_grid(x0, y0, ref, x, y, v, dx, dy, F(Nx + 1, Ny), F(Nx + 1, Ny))
+        got = sf.zeros(*shape)
+        sf.bilinear_marker_to_grid(x0, y0, got, dev(x), dev(y), dev(v), dx, dy)
+        assert np.array_equal(host(got), ref), f"deposit origin ({x0}, {y0})"
+    Vx = np.asfortranarray(rng.normal(size=(Nx + 2, Ny + 1)))
+    Vy = np.asfortranarray(rng.normal(size=(Nx + 1, Ny + 2)))
+    dt = 0.3 * min(dx, dy)
+    xo, yo = x.copy(), y.copy()
+    O.move_markers_rk4(xo, yo, Vx, Vy, o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy)
+    xg, yg = dev(x), dev(y)
+    sf.move_markers_rk4(xg, yg, dev(Vx), dev(Vy), o["x_vx"], o["y_vx"], o["x_vy"], o["y_vy"], dt, lx, ly, dx, dy)
+    assert np.array_equal(host(xg), xo) and np.array_equal(host(yg), yo)
+
+
 def test_advection_bitexact(sf, oracle_lib):
     O = oracle_lib
     Nx, Ny = 41, 35
@@ -238,7 +326,7 @@ def test_rebin_counts_and_order(sf, oracle_lib):
     p = perm.cpu().numpy()[: off[-1]]
     assert off[-1] == nm - 2
     assert np.array_equal(np.sort(p), np.arange(2, nm))
-    for c in range(0, counts_o.size, 97):
+    for c in range(counts_o.size):
         seg = p[off[c]:off[c + 1]]
         assert np.all(np.diff(seg) > 0)
 
