@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "sf_internal.cuh"
@@ -30,6 +31,69 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 
 int set_device(sf_ctx* ctx) {
     SF_CUDA(cudaSetDevice(ctx->device));
+    return SF_OK;
+}
+
+// --------------------------------------------------------------------------
+// peer access between the devices of ranks, and block copies between ranks
+// --------------------------------------------------------------------------
+namespace {
+constexpr int MAX_DEV = 64;
+std::mutex g_peer_mutex;
+signed char g_peer[MAX_DEV][MAX_DEV] = {};   // 0: not asked yet, 1: dev reads / writes peer's memory, -1: cannot
+}
+
+int peer_access(int dev, int peer, bool* ok) {
+    *ok = (dev == peer);
+    if (dev == peer) return SF_OK;
+    if (dev < 0 || peer < 0 || dev >= MAX_DEV || peer >= MAX_DEV) return fail(SF_ERR_NO_DEVICE, "peer_access: device index");
+    std::lock_guard<std::mutex> lock(g_peer_mutex);
+    if (g_peer[dev][peer] == 0) {
+        int can = 0;
+        SF_CUDA(cudaDeviceCanAccessPeer(&can, dev, peer));
+        g_peer[dev][peer] = -1;
+        if (can) {
+            int cur = 0;
+            SF_CUDA(cudaGetDevice(&cur));
+            SF_CUDA(cudaSetDevice(dev));
+            const cudaError_t e = cudaDeviceEnablePeerAccess(peer, 0);
+            if (e == cudaSuccess || e == cudaErrorPeerAccessAlreadyEnabled) {
+                (void)cudaGetLastError();
+                g_peer[dev][peer] = 1;
+            } else {
+                (void)cudaGetLastError();   // not enabled: the copies go through the runtime
+            }
+            SF_CUDA(cudaSetDevice(cur));
+        }
+    }
+    *ok = g_peer[dev][peer] == 1;
+    return SF_OK;
+}
+
+__global__ void k_copy_block(double* __restrict__ dst, int64_t ld_dst, const double* __restrict__ src, int64_t ld_src,
+                             int64_t w, int64_t h) {
+    const int64_t n = w * h;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = k % w, j = k / w;
+        dst[i + j * ld_dst] = src[i + j * ld_src];
+    }
+}
+
+int copy_block(sf_ctx* ctx, cudaStream_t s, double* dst, int64_t ld_dst, const double* src, int64_t ld_src,
+               int64_t w, int64_t h, int src_device) {
+    if (w <= 0 || h <= 0) return SF_OK;
+    bool direct = false;
+    int rc = peer_access(ctx->device, src_device, &direct);
+    if (rc) return rc;
+    if (direct) {
+        const int64_t n = w * h;
+        const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)ctx->num_sms * 8));
+        k_copy_block<<<g, 256, 0, s>>>(dst, ld_dst, src, ld_src, w, h);
+        SF_LAUNCHED(ctx);
+    } else {
+        SF_CUDA(cudaMemcpy2DAsync(dst, (size_t)ld_dst * 8, src, (size_t)ld_src * 8, (size_t)w * 8, (size_t)h,
+                                  cudaMemcpyDefault, s));
+    }
     return SF_OK;
 }
 

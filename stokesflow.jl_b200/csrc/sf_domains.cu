@@ -8,9 +8,12 @@
 //     markers near an edge shared with a neighbour moved to that neighbour.
 //
 // All ranks are driven from one host thread, each on its own context (device
-// and work stream).  Data crosses between ranks as peer copies
-// (cudaMemcpyDefault: NVLink between GPUs, a device copy on one GPU), ordered
-// by events.  Compiled like the other FP64 files (-fmad=false): the one
+// and work stream).  Data crosses between ranks on the receiving rank's
+// device: blocks of the overlap sums by a copy kernel that reads the
+// neighbour's memory directly when the two devices are peers (copy_block,
+// which enables peer access on first use; other pairs go through
+// cudaMemcpy2DAsync), the exchanged markers as contiguous peer copies
+// (cudaMemcpyDefault), all ordered by events.  Compiled like the other FP64 files (-fmad=false): the one
 // arithmetic step of the exchange, x - (lx - dx) * shift, rounds as Julia's.
 #include <algorithm>
 #include <vector>
@@ -231,14 +234,20 @@ int sf_sum_overlapping_values(sf_rank_array* ranks, int32_t dims_x, int32_t dims
             const int l = dim == 0 ? nb(r, -1, 0) : nb(r, 0, -1), u = dim == 0 ? nb(r, 1, 0) : nb(r, 0, 1);
             for (int q : {l, u})
                 if (q >= 0) SF_CUDA(cudaStreamWaitEvent(s, ev[q], 0));
+            // copied on this rank's device, reading the neighbour's memory directly when the devices are peers
             if (dim == 0) {
                 // the lower neighbour's last ox planes, the upper neighbour's first ox planes
-                if (l >= 0) SF_CUDA(cudaMemcpy2DAsync(lo[r], ox * 8, ranks[l].a + (nx - ox), nx * 8, ox * 8, ny,
-                                                      cudaMemcpyDefault, s));
-                if (u >= 0) SF_CUDA(cudaMemcpy2DAsync(hi[r], ox * 8, ranks[u].a, nx * 8, ox * 8, ny, cudaMemcpyDefault, s));
+                if (l >= 0 && (rc = copy_block(k.ctx, s, lo[r], ox, ranks[l].a + (nx - ox), nx, ox, ny,
+                                               ranks[l].ctx->device)))
+                    return rc;
+                if (u >= 0 && (rc = copy_block(k.ctx, s, hi[r], ox, ranks[u].a, nx, ox, ny, ranks[u].ctx->device)))
+                    return rc;
             } else {
-                if (l >= 0) SF_CUDA(cudaMemcpyAsync(lo[r], ranks[l].a + (ny - oy) * nx, nx * oy * 8, cudaMemcpyDefault, s));
-                if (u >= 0) SF_CUDA(cudaMemcpyAsync(hi[r], ranks[u].a, nx * oy * 8, cudaMemcpyDefault, s));
+                if (l >= 0 && (rc = copy_block(k.ctx, s, lo[r], nx, ranks[l].a + (ny - oy) * nx, nx, nx, oy,
+                                               ranks[l].ctx->device)))
+                    return rc;
+                if (u >= 0 && (rc = copy_block(k.ctx, s, hi[r], nx, ranks[u].a, nx, nx, oy, ranks[u].ctx->device)))
+                    return rc;
             }
             SF_CUDA(cudaEventRecord(ev[r], s));
         }
@@ -427,6 +436,9 @@ int sf_exchange_markers(sf_marker_rank* ranks, int32_t dims_x, int32_t dims_y, d
             const int64_t cnt = ws.tot[i];
             if (cnt == 0) continue;
             SF_CUDA(cudaStreamWaitEvent(c->work, ws.ev, 0));
+            // a direct peer copy when the sender's device is a peer of this one (enabled on first use)
+            bool direct = false;
+            if ((rc = peer_access(c->device, ranks[src].ctx->device, &direct))) break;
             const int64_t o = ws.send_base[i];
             SF_CUDA(cudaMemcpyAsync(k.x_out + pos, ws.sx + o, cnt * 8, cudaMemcpyDefault, c->work));
             SF_CUDA(cudaMemcpyAsync(k.y_out + pos, ws.sy + o, cnt * 8, cudaMemcpyDefault, c->work));

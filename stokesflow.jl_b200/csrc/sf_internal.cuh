@@ -90,6 +90,15 @@ namespace sf {
 // Ensures `s` holds at least `bytes`; contents are not preserved.
 int ensure(sf_ctx* ctx, Scratch& s, size_t bytes);
 int set_device(sf_ctx* ctx);
+// Whether device `dev` can read and write `peer`'s memory directly (NVLink / PCIe peer access), enabling it on
+// first use; *ok is true for dev == peer.  Pairs without peer access copy through the runtime instead.
+int peer_access(int dev, int peer, bool* ok);
+// A w x h block of doubles (rows of w contiguous entries, leading dimensions ld_dst / ld_src) from src, which
+// lives on src_device, to dst on ctx's device, queued on stream s of that device (current).  With peer access
+// (or one device) a copy kernel on ctx's device reads src directly -- plain loads, no multicast; otherwise
+// cudaMemcpy2DAsync does it.
+int copy_block(sf_ctx* ctx, cudaStream_t s, double* dst, int64_t ld_dst, const double* src, int64_t ld_src,
+               int64_t w, int64_t h, int src_device);
 // frees the context's cached batch engine (sf_mixed.cu)
 void mixed_engine_release(sf_ctx* ctx);
 

@@ -879,24 +879,26 @@ static int halo_dimension(std::vector<Rank>& R, const std::vector<HaloArray>& ar
         Rank& b = R[up];
         for (const HaloArray& h : arrays) {
             const int64_t nx = Nx + h.sx, ny = Ny + h.sy, n = dim == 0 ? nx : ny, ol = 2 + (dim == 0 ? h.sx : h.sy);
-            // into b's first plane from a's plane n-ol, on b's stream once a's phase is done
-            auto plane = [&](const double* src, int64_t ld_src, int64_t i_src, double* dst, int64_t ld_dst,
-                             int64_t i_dst, cudaStream_t s) -> int {
+            // one plane: an x plane is a column of ny entries ld apart, a y plane a row of nx contiguous entries;
+            // copied on the receiving rank's device, reading the sender's memory directly when the devices are
+            // peers (copy_block)
+            auto plane = [&](Rank& from, const double* src, int64_t ld_src, int64_t i_src, Rank& to, double* dst,
+                             int64_t ld_dst, int64_t i_dst) -> int {
                 if (dim == 0)
-                    SF_CUDA(cudaMemcpy2DAsync(dst + i_dst, ld_dst * 8, src + i_src, ld_src * 8, 8, ny,
-                                              cudaMemcpyDefault, s));
-                else
-                    SF_CUDA(cudaMemcpyAsync(dst + i_dst * ld_dst, src + i_src * ld_src, nx * 8, cudaMemcpyDefault, s));
-                return SF_OK;
+                    return copy_block(to.ctx, to.s, dst + i_dst, ld_dst, src + i_src, ld_src, 1, ny,
+                                      from.ctx->device);
+                return copy_block(to.ctx, to.s, dst + i_dst * ld_dst, ld_dst, src + i_src * ld_src, ld_src, nx, 1,
+                                  from.ctx->device);
             };
             int rc;
+            // into b's first plane from a's plane n-ol, on b's stream once a's phase is done
             SF_CUDA(cudaSetDevice(b.ctx->device));
             SF_CUDA(cudaStreamWaitEvent(b.s, a.ev, 0));
-            if ((rc = plane(h.p[r], h.ld[r], n - ol, h.p[up], h.ld[up], 0, b.s))) return rc;
+            if ((rc = plane(a, h.p[r], h.ld[r], n - ol, b, h.p[up], h.ld[up], 0))) return rc;
             // into a's last plane from b's plane ol-1, on a's stream once b's phase is done
             SF_CUDA(cudaSetDevice(a.ctx->device));
             SF_CUDA(cudaStreamWaitEvent(a.s, b.ev, 0));
-            if ((rc = plane(h.p[up], h.ld[up], ol - 1, h.p[r], h.ld[r], n - 1, a.s))) return rc;
+            if ((rc = plane(b, h.p[up], h.ld[up], ol - 1, a, h.p[r], h.ld[r], n - 1))) return rc;
         }
     }
     for (Rank& k : R) {  // this dimension's incoming planes are in place

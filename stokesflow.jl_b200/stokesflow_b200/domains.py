@@ -227,13 +227,27 @@ def initialize_markers_decomposed(dims, Nx: int, Ny: int, Lx: float, Ly: float, 
     return out
 
 
+def rank_devices(dims, n_devices: int) -> dict:
+    """Devices for a dims[0] x dims[1] grid of ranks on n_devices GPUs: {(cx, cy): device index}.  The ranks
+    are taken in MPI rank order of the Cartesian communicator (x slowest, rank = cx * dims[1] + cy) and cut
+    into n_devices contiguous runs of near-equal length (sizes differ by at most one), so that the ranks
+    sharing a GPU are y-neighbours and a halo update crosses between GPUs only at the runs' ends.  With more
+    devices than ranks every rank has a GPU of its own."""
+    if n_devices < 1:
+        raise ValueError("rank_devices: need at least one device")
+    n = dims[0] * dims[1]
+    return {(cx, cy): (cx * dims[1] + cy) * n_devices // n for cx in range(dims[0]) for cy in range(dims[1])}
+
+
 class DecomposedStokesFlow2D:
     """The StokesFlow2D timestep loop (StokesFlow2D_multixpu.jl:157-191) on dims[0] x dims[1] ranks driven from
     this process: per timestep the three deposits with overlap sums, the decomposed solve, RK4 advection of
     each rank's markers on its local domain, and the marker exchange.  Nx, Ny: local grid points of a rank;
     Lx, Ly: the global domain.  markers {(cx, cy): (x_m, y_m, rho_m, mu_m)} in local coordinates (the ranks'
     initial markers), or None to lay them out from ``model`` with :func:`initialize_markers_decomposed`;
-    devices {(cx, cy): CUDA device index} (default: the current device for all)."""
+    devices {(cx, cy): CUDA device index}, or "auto" for :func:`rank_devices` over every visible GPU (default:
+    the current device for all).  Halo planes and overlap blocks between ranks on different GPUs are read
+    directly from the neighbour's memory where the two GPUs are peers (NVLink), else copied by the runtime."""
 
     def __init__(self, dims, Nx: int, Ny: int, Lx: float, Ly: float, markers: dict | None = None, *, model=None,
                  marker_density: int = 4, jitter: float = 0.0, seed: int = 0, eps=1e-5, iter_max=100000,
@@ -249,6 +263,8 @@ class DecomposedStokesFlow2D:
         self.dt, self.t_tot, self.nt = 0.0, 0.0, 0
         self.ctx, self.ranks, self.sums = {}, {}, {}
         coords = [(cx, cy) for cy in range(dims[1]) for cx in range(dims[0])]
+        if devices == "auto":
+            devices = rank_devices(dims, torch.cuda.device_count())
         for c in coords:
             dev = (devices or {}).get(c, torch.cuda.current_device())
             with torch.cuda.device(dev):

@@ -204,3 +204,19 @@ def test_reference_marker_to_grid_multi_process():
         multi = domains.gather(local[name], name, dims, Nx, Ny).numpy()
         assert multi.shape == single.shape
         assert np.all(np.abs(multi - single) <= tol * np.maximum(np.abs(multi), np.abs(single))), name   # :141-143
+
+
+@pytest.mark.parametrize("dims, n_dev", [((3, 2), 4), ((2, 2), 2), ((1, 3), 8), ((4, 4), 8), ((5, 3), 4)])
+def test_rank_devices_are_contiguous_balanced_runs(dims, n_dev):
+    """The rank -> GPU assignment of the decomposition: contiguous runs in MPI rank order (x slowest), run
+    lengths differing by at most one, every GPU used when there are at least as many ranks, one rank per GPU
+    otherwise, and the same answer every time."""
+    from stokesflow_b200.domains import rank_devices
+    a = rank_devices(dims, n_dev)
+    assert a == rank_devices(dims, n_dev)
+    order = [a[(cx, cy)] for cx in range(dims[0]) for cy in range(dims[1])]   # MPI rank order
+    n = dims[0] * dims[1]
+    assert order == sorted(order) and all(0 <= d < n_dev for d in order)
+    sizes = [order.count(d) for d in sorted(set(order))]
+    assert max(sizes) - min(sizes) <= 1
+    assert len(set(order)) == min(n, n_dev)
