@@ -97,7 +97,9 @@ def parse():
                     help="default line without the bounded precision / batch / serve forms object")
     ap.add_argument("--forms-batch", type=int, default=64, help="forms object: batch instances")
     ap.add_argument("--forms-requests", type=int, default=16, help="forms object: serve requests")
-    ap.add_argument("--forms-rate", type=float, default=4.0, help="forms object: serve requests per second")
+    ap.add_argument("--forms-rate", type=float, default=16.0,
+                    help="forms object: serve requests per second (above both servers' capacity, so that solves/s "
+                         "measures throughput, not the arrival rate)")
     ap.add_argument("--forms-cells", default="63,511", help="forms object: serve cells per side")
     ap.add_argument("--forms-precision-n", type=int, default=1024, help="forms object: precision grid points")
     ap.add_argument("--forms-precision-steps", type=int, default=3, help="forms object: precision timesteps")

@@ -161,3 +161,65 @@ def test_summary_of_the_served_trace(server):
     assert out["completed"] == 8 and out["solves"] == sum(1 + k % 3 for k in range(8))
     assert 0 < out["p50_latency_s"] <= out["p99_latency_s"]
     assert all(r.t_admit >= r.arrival and r.t_done >= r.t_admit for r in reqs)
+
+
+def _concurrent_fakes(monkeypatch):
+    """Fakes for the plain FP64 server's workers: no device, a request 'solve' is a sleep."""
+    import contextlib
+    import threading
+
+    class Ctx:
+        def __init__(self, device=None):
+            pass
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(serving.api, "default_context", lambda: object())
+    monkeypatch.setattr(serving.api, "Context", Ctx)
+    monkeypatch.setattr(serving.torch.cuda, "current_device", lambda: 0)
+    monkeypatch.setattr(serving.torch.cuda, "set_device", lambda d: None)
+    monkeypatch.setattr(serving.torch.cuda, "Stream", lambda: None)
+    monkeypatch.setattr(serving.torch.cuda, "stream", lambda s: contextlib.nullcontext())
+    monkeypatch.setattr(serving.torch.cuda, "synchronize", lambda d=None: None)
+    lock = threading.Lock()
+    seen = {"running": 0, "peak": 0, "starts": []}
+
+    def serve(self, r, ctx=None):
+        with lock:
+            seen["running"] += 1
+            seen["peak"] = max(seen["peak"], seen["running"])
+            seen["starts"].append(r.rid)
+        time.sleep(0.02 * r.timesteps)
+        r.solves = r.converged = r.timesteps
+        with lock:
+            seen["running"] -= 1
+
+    monkeypatch.setattr(serving.StokesServer, "_serve_fp64", serve)
+    return seen
+
+
+def test_concurrent_fp64_server_keeps_order_workers_and_budget(monkeypatch):
+    """The plain FP64 server with K workers: requests start in arrival order, at most K run at once, the HBM
+    budget bounds the state held, and every request completes once."""
+    seen = _concurrent_fakes(monkeypatch)
+    reqs = [request(k, 33, 1 + k % 3, 0.005 * k) for k in range(9)]
+    srv = serving.StokesServer(1 << 40, solver="fp64", concurrency=3)
+    out = srv.run(reqs)
+    assert out["completed"] == 9 and out["solves"] == sum(1 + k % 3 for k in range(9))
+    assert seen["starts"] == list(range(9)) and seen["peak"] == 3
+    assert srv.state_used == 0 and all(r.t_done >= r.t_admit >= r.arrival for r in reqs)
+
+    seen = _concurrent_fakes(monkeypatch)
+    reqs = [request(k, 33, 2, 0.0) for k in range(6)]
+    one = serving.state_bytes(reqs[0].spec)
+    srv = serving.StokesServer(2 * one, solver="fp64", concurrency=4)     # room for two requests' state
+    out = srv.run(reqs)
+    assert out["completed"] == 6 and seen["peak"] == 2 and srv.peak_state == 2 * one
+
+
+def test_concurrency_only_for_the_fp64_server():
+    with pytest.raises(ValueError):
+        serving.StokesServer(1 << 30, solver="mixed", concurrency=2)
+    with pytest.raises(ValueError):
+        serving.StokesServer(1 << 30, solver="fp64", concurrency=0)
