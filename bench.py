@@ -840,7 +840,10 @@ def run_reference(a, rank):
                                        f"{a.n}^2 solve, OpenMP over {n} threads",
                              "cpu": _cpu_model(), "detail": dets},
             "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "gpu_launches": 0}
+            "gpu_launches": 0,
+            "note": "a step here is one bounded sample (one grid's serial deposit, then the PT iterations above), "
+                    "timed on the host cores; value is the sample's PT T_eff (the deposit is outside it), so "
+                    "ms_per_step is not a timestep"}
 
 
 # ---------------------------------------------------------------------------
