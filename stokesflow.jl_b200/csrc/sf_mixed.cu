@@ -1495,7 +1495,13 @@ int engine_round(sf_engine* e, cudaStream_t caller) {
     }
     if (!swept.empty()) {  // V += dV, P += dP for every instance that ran sweeps
         SF_CUDA(cudaMemcpyAsync(e->d_list, swept.data(), swept.size() * 4, cudaMemcpyHostToDevice, s));
-        k_accumulate<<<dim3(64, (unsigned)swept.size()), 256, 0, s>>>(e->d_insts, e->d_ctl, e->d_list);
+        // blocks per instance: enough to cover the largest one, at least 64, the whole launch around 8 per SM
+        int64_t most = 0;
+        for (int q : swept) most = std::max(most, e->slots[q].d.LD32 * e->slots[q].d.rows);
+        const int64_t gx = std::max<int64_t>(
+            1, std::min<int64_t>(ceil_div(most, 256),
+                                 std::max<int64_t>(64, (int64_t)ctx->num_sms * 8 / (int64_t)swept.size())));
+        k_accumulate<<<dim3((unsigned)gx, (unsigned)swept.size()), 256, 0, s>>>(e->d_insts, e->d_ctl, e->d_list);
         SF_LAUNCHED(ctx);
     }
     k_resid64<<<(unsigned)nt, T64, 0, s>>>(e->d_insts, e->d_tiles64, e->d_part);
