@@ -275,59 +275,106 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_cells(const int32_t* __re
 // node (ix, iy) with (1-dx)(1-dy), (ix+1, iy) with dx(1-dy), (ix, iy+1) with (1-dx)dy and (ix+1, iy+1) with dx*dy
 // (MarkerToGrid.jl:124-151), so node (I, J) merges the cells (I,J), (I-1,J), (I,J-1), (I-1,J-1), whose records
 // are sorted by marker index: taking the smallest head each time visits the node's markers in ascending
-// index order, the reference's serial order.  The records of neighbouring cells are neighbours in memory, so
-// the threads of a warp (neighbouring nodes of a grid row) walk overlapping, contiguous runs of records.
-__global__ void __launch_bounds__(DEP_THREADS) k_gather_sorted(const Payload* __restrict__ pl,
+// index order, the reference's serial order.
+//
+// Each list's head record is held in registers, so a visit reads its record once, with one 32-byte load (the
+// four threads that use a record read it from L2).  The merge gallops: once the smallest head is chosen, the
+// records of its list that stay below the other lists' smallest head are the merge's next picks, in order,
+// and are taken in an inner loop without comparing the four heads again.  Markers keep much of their initial
+// lattice order, so these runs are several records long.
+constexpr int GT_NONE = 0x7fffffff;   // head of an exhausted list
+constexpr int GT_X = 32, GT_Y = 4;    // nodes of a block: one warp per node row, 4 rows that share cell rows
+// (launched 8 blocks per SM: 64 registers, more warps in flight than a spill-free 68)
+
+__global__ void __launch_bounds__(GT_X * GT_Y, 8) k_gather_sorted(const Payload* __restrict__ pl,
                                                                const int32_t* __restrict__ offsets, int64_t nx,
                                                                int64_t ny, double* __restrict__ val_grid,
                                                                double* __restrict__ val_wt_sum,
                                                                double* __restrict__ wt_sum, int64_t ld_sum,
                                                                unsigned long long* __restrict__ empty_counter) {
-    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (n >= nx * ny) return;
-    const int64_t I = n % nx + 1, J = n / nx + 1;
+    const int64_t ntx = (nx + GT_X - 1) / GT_X;
+    const int64_t I = (int64_t)(blockIdx.x % ntx) * GT_X + (threadIdx.x % GT_X) + 1;
+    const int64_t J = (int64_t)(blockIdx.x / ntx) * GT_Y + (threadIdx.x / GT_X) + 1;
+    if (I > nx || J > ny) return;
     const int64_t ldc = nx + 1;
-    int32_t cur[4], end[4], head[4];
     // corner k: 0 = marker's top-left node (cell I,J), 1 = top-right (cell I-1,J),
     //           2 = bottom-left (cell I,J-1), 3 = bottom-right (cell I-1,J-1)
+    int32_t cur[4], end[4], hm[4];
+    double hdx[4], hdy[4], hv[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int64_t key = (I - (k & 1)) + (J - (k >> 1)) * ldc;
         cur[k] = offsets[key];
         end[k] = offsets[key + 1];
-        head[k] = (cur[k] < end[k]) ? pl[cur[k]].m : 0x7fffffff;
+        hdx[k] = hdy[k] = hv[k] = 0.0;
+        hm[k] = GT_NONE;
+        if (cur[k] < end[k]) {
+            const Payload p = pl[cur[k]];
+            hdx[k] = p.dxij;
+            hdy[k] = p.dyij;
+            hv[k] = p.val;
+            hm[k] = p.m;
+        }
     }
     double ws = 0.0, vs = 0.0;
     while (true) {
         int kb = 0;
-        int32_t best = head[0];
+        int32_t best = hm[0];
 #pragma unroll
         for (int k = 1; k < 4; ++k)
-            if (head[k] < best) {
-                best = head[k];
+            if (hm[k] < best) {
+                best = hm[k];
                 kb = k;
             }
-        if (best == 0x7fffffff) break;
-        int32_t pos = 0;
+        if (best == GT_NONE) break;
+        int32_t t = GT_NONE;   // the smallest head of the other lists
+        int32_t c = 0, e = 0;
+        double dx = 0.0, dy = 0.0, v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (k != kb && hm[k] < t) t = hm[k];
+            if (k == kb) {
+                c = cur[k];
+                e = end[k];
+                dx = hdx[k];
+                dy = hdy[k];
+                v = hv[k];
+            }
+        }
+        const bool fx = kb & 1, fy = kb >> 1;
+        int32_t h;
+        do {   // list kb's run below t
+            const double wx = fx ? dx : (1.0 - dx);
+            const double wy = fy ? dy : (1.0 - dy);
+            const double w = wx * wy;
+            ws = ws + w;
+            vs = vs + w * v;
+            ++c;
+            h = GT_NONE;
+            if (c < e) {
+                const Payload p = pl[c];
+                dx = p.dxij;
+                dy = p.dyij;
+                v = p.val;
+                h = p.m;
+            }
+        } while (h < t);
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (k == kb) {
-                pos = cur[k]++;
-                head[k] = (cur[k] < end[k]) ? pl[cur[k]].m : 0x7fffffff;
+                cur[k] = c;
+                hm[k] = h;
+                hdx[k] = dx;
+                hdy[k] = dy;
+                hv[k] = v;
             }
-        const Payload p = pl[pos];
-        const double wx = (kb & 1) ? p.dxij : (1.0 - p.dxij);
-        const double wy = (kb >> 1) ? p.dyij : (1.0 - p.dyij);
-        const double w = wx * wy;
-        ws = ws + w;
-        vs = vs + w * p.val;
     }
     if (wt_sum) {
         wt_sum[(I - 1) + (J - 1) * ld_sum] = ws;
         val_wt_sum[(I - 1) + (J - 1) * ld_sum] = vs;
     }
     if (ws != 0.0)
-        val_grid[(I - 1) + (J - 1) * nx] = vs / ws;
+        val_grid[(I - 1) + (J - 1) * nx] = vs / ws;   // safeDivision (MarkerToGrid.jl:164-172)
     else if (empty_counter)
         atomicAdd(empty_counter, 1ull);
 }
@@ -472,7 +519,7 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
         SF_CUDA(cudaMemsetAsync(wt_sum, 0, (size_t)n_sum * 8, s));
         SF_CUDA(cudaMemsetAsync(val_wt_sum, 0, (size_t)n_sum * 8, s));
     }
-    k_gather_sorted<<<(unsigned)ceil_div(nx * ny, DEP_THREADS), DEP_THREADS, 0, s>>>(
+    k_gather_sorted<<<(unsigned)(ceil_div(nx, GT_X) * ceil_div(ny, GT_Y)), GT_X * GT_Y, 0, s>>>(
         (const Payload*)ctx->payload.ptr, (const int32_t*)ctx->offsets.ptr, nx, ny, val_grid, val_wt_sum, wt_sum,
         ld_sum, ctx->d_counters + CNT_EMPTY_NODES);
     SF_LAUNCHED(ctx);
