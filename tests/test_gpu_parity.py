@@ -101,6 +101,46 @@ def test_deposit_clustered_markers(sf, oracle_lib):
     assert np.array_equal(host(got), ref)
 
 
+@pytest.mark.parametrize("order", ["x_fastest", "y_fastest", "reversed", "cell_blocks", "alternating_rows"])
+def test_deposit_marker_orders(sf, oracle_lib, order):
+    """A jittered lattice of 5x5 markers per cell in orders that give the gather's merge long runs from one
+    cell (cell blocks), runs that alternate between neighbouring cells (lattice rows), and runs in reverse
+    order; all three staggered grids, bit for bit against the oracle's serial loop."""
+    O = oracle_lib
+    Nx, Ny = 26, 19
+    dx, dy = 1.0 / (Nx - 1), 0.7 / (Ny - 1)
+    k = 5
+    mx, my = (Nx - 1) * k, (Ny - 1) * k
+    rng = np.random.default_rng(21)
+    ii, jj = np.meshgrid(np.arange(mx), np.arange(my), indexing="ij")    # ii: x index, jj: y index
+    x = (ii + 0.5 + 0.4 * (rng.random(ii.shape) - 0.5)) * dx / k
+    y = (jj + 0.5 + 0.4 * (rng.random(jj.shape) - 0.5)) * dy / k
+    if order == "x_fastest":
+        idx = np.ravel_multi_index((ii.T.ravel(), jj.T.ravel()), ii.shape)
+    elif order == "y_fastest":
+        idx = np.arange(ii.size)
+    elif order == "reversed":
+        idx = np.ravel_multi_index((ii.T.ravel(), jj.T.ravel()), ii.shape)[::-1]
+    elif order == "cell_blocks":
+        cell = (ii // k) + (jj // k) * (Nx - 1)
+        idx = np.argsort(cell.ravel(), kind="stable")
+    else:   # lattice rows in x order, every second row reversed
+        rows = [np.ravel_multi_index((np.arange(mx)[::(1 if j % 2 == 0 else -1)], np.full(mx, j)), ii.shape)
+                for j in range(my)]
+        idx = np.concatenate(rows)
+    x, y = x.ravel()[idx], y.ravel()[idx]
+    v = np.exp(rng.normal(size=x.size))
+    o = O.node_origins(dx, dy)
+    xt, yt, vt = dev(x), dev(y), dev(v)
+    for x0, y0, shape in ((o["x_rho"], o["y_rho"], (Nx + 1, Ny)), (o["x"], o["y"], (Nx, Ny)),
+                          (o["x_p"], o["y_p"], (Nx - 1, Ny - 1))):
+        ref = F(*shape)
+        O.bilinear_marker_to_grid(x0, y0, ref, x, y, v, dx, dy, F(Nx + 1, Ny), F(Nx + 1, Ny))
+        got = sf.zeros(*shape)
+        sf.bilinear_marker_to_grid(x0, y0, got, xt, yt, vt, dx, dy)
+        assert np.array_equal(host(got), ref), (order, shape)
+
+
 def test_deposit_and_rebin_with_markers_piled_in_one_cell(sf, oracle_lib):
     """Markers piled into single cells, as markers clamped into a corner pile up: one cell holds 10^5 markers
     (more than a shared-memory window of the segment sort), another 2000, the rest of the grid ~25 per cell,
