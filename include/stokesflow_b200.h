@@ -92,6 +92,27 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
                                double* val_wt_sum, double* wt_sum, int64_t ld_sum, int64_t n_sum,
                                void* stream);
 
+/* The deposits of one StokesFlow2D timestep in one call (the three calls of
+ * StokesFlow2D_multixpu.jl:164-166: rho_vy, mu_b, mu_p): up to SF_MAX_GRIDS
+ * grids over the same markers, each with its own origin, extents, output and
+ * marker values.  The result is that of sf_bilinear_marker_to_grid called once
+ * per grid in the given order, bit for bit: each grid as described there, the
+ * warning counters summed over the grids, and val_wt_sum / wt_sum (optional,
+ * large enough for every grid) holding the last grid's sums.  The markers'
+ * positions are read once for all grids' cell assignments.  All arguments are
+ * checked before any work starts. */
+#define SF_MAX_GRIDS 4
+typedef struct {
+    double x_grid_min, y_grid_min;
+    double* val_grid;        /* (nx, ny), column-major                              */
+    int64_t nx, ny;
+    const double* val_m;     /* the marker values deposited onto this grid          */
+} sf_deposit_grid;
+int sf_bilinear_marker_to_grids(sf_ctx* ctx, const sf_deposit_grid* grids, int n_grids,
+                                const double* x_m, const double* y_m, int64_t nm, double dx, double dy,
+                                double* val_wt_sum, double* wt_sum, int64_t ld_sum, int64_t n_sum,
+                                void* stream);
+
 /* Allocation-free deposit.  No counterpart in the reference: it is
  * sf_bilinear_marker_to_grid (same result, bit for bit) for callers that cannot
  * let a library allocate device memory -- a host runtime that owns the GPU

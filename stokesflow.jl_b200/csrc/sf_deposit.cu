@@ -79,6 +79,47 @@ __global__ void k_cell_keys(const double* __restrict__ x, const double* __restri
     }
 }
 
+// 1 for several grids over the same markers (the three deposits of a timestep): each marker's position is read
+// once, and every grid gets its own keys and counts, exactly as k_cell_keys computes them.
+struct GridKeys {
+    double xmin[SF_MAX_GRIDS], ymin[SF_MAX_GRIDS];
+    int64_t nx[SF_MAX_GRIDS], ny[SF_MAX_GRIDS];
+    int32_t* keys[SF_MAX_GRIDS];
+    int32_t* counts[SF_MAX_GRIDS];
+    int n;
+};
+
+__global__ void k_cell_keys_grids(const double* __restrict__ x, const double* __restrict__ y, int64_t nm, double dx,
+                                  double dy, const GridKeys g, unsigned long long* __restrict__ bad_counter) {
+    const int lane = threadIdx.x & 31;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < nm; base += stride) {
+        const int64_t m = base + threadIdx.x;
+        const bool live = m < nm;
+        const double xm = live ? x[m] : 0.0, ym = live ? y[m] : 0.0;
+        const unsigned active = __ballot_sync(0xffffffffu, live);
+#pragma unroll
+        for (int k = 0; k < SF_MAX_GRIDS; ++k) {
+            if (k >= g.n) break;
+            if (!live) continue;
+            int32_t key = -1;
+            const TopLeft t = topleft(g.xmin[k], g.ymin[k], xm, ym, dx, dy);
+            // MarkerToGrid.jl:66: accept iff 0 <= ix <= Nx && 0 <= iy <= Ny (ix = qx + 1)
+            if (t.qx >= -1.0 && t.qx <= (double)(g.nx[k] - 1) && t.qy >= -1.0 && t.qy <= (double)(g.ny[k] - 1))
+                key = (int32_t)((int64_t)t.qx + 1 + ((int64_t)t.qy + 1) * (g.nx[k] + 1));
+            g.keys[k][m] = key;
+            const unsigned peers = __match_any_sync(active, key);
+            if (lane == __ffs(peers) - 1) {
+                const int n = __popc(peers);
+                if (key >= 0)
+                    atomicAdd(&g.counts[k][key], n);
+                else if (bad_counter)
+                    atomicAdd(bad_counter, (unsigned long long)n);
+            }
+        }
+    }
+}
+
 // 3. scatter marker indices into their cells (order within a cell arbitrary).
 __global__ void k_scatter(const int32_t* __restrict__ keys, int64_t nm, const int32_t* __restrict__ offsets,
                           int32_t* __restrict__ cursor, int32_t* __restrict__ perm) {
@@ -442,34 +483,25 @@ static unsigned grid_for(sf_ctx* ctx, int64_t n, int threads) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, threads), (int64_t)ctx->num_sms * 32));
 }
 
-// Steps 1-4: stable counting sort of markers by cell -> ctx->counts / offsets, and either the cell-ordered
-// permutation in ctx->perm or (with val) the cell-ordered payload records in ctx->payload.
-static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, const double* val, int64_t nm, double xmin,
-                        double ymin, double dx, double dy, int64_t nx, int64_t ny, unsigned long long* bad_counter,
-                        cudaStream_t s) {
+// Steps 2-4 from cell keys and per-cell counts already computed (step 1): the stable counting sort of markers by
+// cell -> ctx->offsets, and either the cell-ordered permutation in ctx->perm or (with val) the cell-ordered
+// payload records in ctx->payload.  keys is spent afterwards: it is the radix sort's second buffer.
+static int sort_from_keys(sf_ctx* ctx, int32_t* keys, const int32_t* counts, const double* x, const double* y,
+                          const double* val, int64_t nm, double xmin, double ymin, double dx, double dy, int64_t nx,
+                          int64_t ny, cudaStream_t s) {
     int64_t ncells = (nx + 1) * (ny + 1);
     int rc;
-    if ((rc = ensure(ctx, ctx->keys, (size_t)std::max<int64_t>(nm, 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->perm, (size_t)std::max<int64_t>(nm, 1) * 4))) return rc;
-    if ((rc = ensure(ctx, ctx->counts, (size_t)(ncells + 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->offsets, (size_t)(ncells + 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->cursor, (size_t)(ncells + 1) * 4))) return rc;
     if ((rc = ensure(ctx, ctx->longs, (size_t)(ncells + 1) * 4))) return rc;
     if (val && (rc = ensure(ctx, ctx->payload, (size_t)std::max<int64_t>(nm, 1) * sizeof(Payload)))) return rc;
-    int32_t* keys = (int32_t*)ctx->keys.ptr;
-    int32_t* counts = (int32_t*)ctx->counts.ptr;
     int32_t* offsets = (int32_t*)ctx->offsets.ptr;
     int32_t* cursor = (int32_t*)ctx->cursor.ptr;
     int32_t* perm = (int32_t*)ctx->perm.ptr;
     int32_t* n_long = (int32_t*)ctx->longs.ptr;   // the count, then the list
-    SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(cursor, 0, (size_t)(ncells + 1) * 4, s));
     SF_CUDA(cudaMemsetAsync(n_long, 0, 4, s));
-    if (nm > 0) {
-        k_cell_keys<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(x, y, nm, xmin, ymin, dx, dy, nx, ny, keys,
-                                                                             counts, bad_counter);
-        SF_LAUNCHED(ctx);
-    }
     if ((rc = exclusive_scan_i32(ctx, counts, offsets, ncells, offsets + ncells, s))) return rc;
     if (nm > 0) {
         k_scatter<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(keys, nm, offsets, cursor, perm);
@@ -489,6 +521,32 @@ static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, const dou
         SF_LAUNCHED(ctx);
     }
     return SF_OK;
+}
+
+// Steps 1-4 for one grid: cell keys and counts into ctx->keys / ctx->counts, then the sort.
+static int sort_by_cell(sf_ctx* ctx, const double* x, const double* y, const double* val, int64_t nm, double xmin,
+                        double ymin, double dx, double dy, int64_t nx, int64_t ny, unsigned long long* bad_counter,
+                        cudaStream_t s) {
+    int64_t ncells = (nx + 1) * (ny + 1);
+    int rc;
+    if ((rc = ensure(ctx, ctx->keys, (size_t)std::max<int64_t>(nm, 1) * 4))) return rc;
+    if ((rc = ensure(ctx, ctx->counts, (size_t)(ncells + 1) * 4))) return rc;
+    int32_t* keys = (int32_t*)ctx->keys.ptr;
+    int32_t* counts = (int32_t*)ctx->counts.ptr;
+    SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)(ncells + 1) * 4, s));
+    if (nm > 0) {
+        k_cell_keys<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(x, y, nm, xmin, ymin, dx, dy, nx, ny, keys,
+                                                                             counts, bad_counter);
+        SF_LAUNCHED(ctx);
+    }
+    return sort_from_keys(ctx, keys, counts, x, y, val, nm, xmin, ymin, dx, dy, nx, ny, s);
+}
+
+static void launch_gather(sf_ctx* ctx, int64_t nx, int64_t ny, double* val_grid, double* val_wt_sum, double* wt_sum,
+                          int64_t ld_sum, cudaStream_t s) {
+    k_gather_sorted<<<(unsigned)(ceil_div(nx, GT_X) * ceil_div(ny, GT_Y)), GT_X * GT_Y, 0, s>>>(
+        (const Payload*)ctx->payload.ptr, (const int32_t*)ctx->offsets.ptr, nx, ny, val_grid, val_wt_sum, wt_sum,
+        ld_sum, ctx->d_counters + CNT_EMPTY_NODES);
 }
 
 }  // namespace sf
@@ -519,10 +577,71 @@ int sf_bilinear_marker_to_grid(sf_ctx* ctx, double x_grid_min, double y_grid_min
         SF_CUDA(cudaMemsetAsync(wt_sum, 0, (size_t)n_sum * 8, s));
         SF_CUDA(cudaMemsetAsync(val_wt_sum, 0, (size_t)n_sum * 8, s));
     }
-    k_gather_sorted<<<(unsigned)(ceil_div(nx, GT_X) * ceil_div(ny, GT_Y)), GT_X * GT_Y, 0, s>>>(
-        (const Payload*)ctx->payload.ptr, (const int32_t*)ctx->offsets.ptr, nx, ny, val_grid, val_wt_sum, wt_sum,
-        ld_sum, ctx->d_counters + CNT_EMPTY_NODES);
+    launch_gather(ctx, nx, ny, val_grid, val_wt_sum, wt_sum, ld_sum, s);
     SF_LAUNCHED(ctx);
+    return SF_OK;
+}
+
+int sf_bilinear_marker_to_grids(sf_ctx* ctx, const sf_deposit_grid* grids, int n_grids, const double* x_m,
+                                const double* y_m, int64_t nm, double dx, double dy, double* val_wt_sum,
+                                double* wt_sum, int64_t ld_sum, int64_t n_sum, void* stream) {
+    SF_REQUIRE(ctx, "sf_bilinear_marker_to_grids: ctx is NULL");
+    SF_REQUIRE(grids && n_grids >= 1 && n_grids <= SF_MAX_GRIDS, "sf_bilinear_marker_to_grids: 1 to SF_MAX_GRIDS grids");
+    SF_REQUIRE(nm >= 0 && (nm == 0 || (x_m && y_m)), "sf_bilinear_marker_to_grids: bad markers");
+    SF_REQUIRE(nm < (int64_t)INT32_MAX, "sf_bilinear_marker_to_grids: more than 2^31-1 markers");
+    SF_REQUIRE(dx > 0.0 && dy > 0.0, "sf_bilinear_marker_to_grids: dx, dy must be positive");
+    SF_REQUIRE((val_wt_sum == nullptr) == (wt_sum == nullptr), "sf_bilinear_marker_to_grids: give both sum arrays or neither");
+    int64_t total_cells = 0;
+    for (int g = 0; g < n_grids; ++g) {
+        const sf_deposit_grid& d = grids[g];
+        SF_REQUIRE(d.val_grid && d.nx >= 1 && d.ny >= 1, "sf_bilinear_marker_to_grids: bad grid");
+        SF_REQUIRE(nm == 0 || d.val_m, "sf_bilinear_marker_to_grids: bad marker values");
+        SF_REQUIRE((d.nx + 1) * (d.ny + 1) < (int64_t)INT32_MAX, "sf_bilinear_marker_to_grids: grid too large");
+        if (wt_sum)
+            SF_REQUIRE(ld_sum >= d.nx && n_sum >= ld_sum * (d.ny - 1) + d.nx,
+                       "sf_bilinear_marker_to_grids: sum arrays too small");
+        total_cells += (d.nx + 1) * (d.ny + 1) + 1;
+    }
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    cudaStream_t s = as_stream(stream);
+    const int64_t nmk = std::max<int64_t>(nm, 1);
+    if ((rc = ensure(ctx, ctx->keys, (size_t)(n_grids * nmk) * 4))) return rc;
+    if ((rc = ensure(ctx, ctx->counts, (size_t)total_cells * 4))) return rc;
+    int32_t* keys = (int32_t*)ctx->keys.ptr;
+    int32_t* counts = (int32_t*)ctx->counts.ptr;
+    SF_CUDA(cudaMemsetAsync(counts, 0, (size_t)total_cells * 4, s));
+    GridKeys gk{};
+    gk.n = n_grids;
+    int64_t off = 0;
+    for (int g = 0; g < n_grids; ++g) {
+        gk.xmin[g] = grids[g].x_grid_min;
+        gk.ymin[g] = grids[g].y_grid_min;
+        gk.nx[g] = grids[g].nx;
+        gk.ny[g] = grids[g].ny;
+        gk.keys[g] = keys + g * nmk;
+        gk.counts[g] = counts + off;
+        off += (grids[g].nx + 1) * (grids[g].ny + 1) + 1;
+    }
+    if (nm > 0) {
+        k_cell_keys_grids<<<grid_for(ctx, nm, DEP_THREADS), DEP_THREADS, 0, s>>>(x_m, y_m, nm, dx, dy, gk,
+                                                                                   ctx->d_counters + CNT_BAD_MARKERS);
+        SF_LAUNCHED(ctx);
+    }
+    for (int g = 0; g < n_grids; ++g) {
+        const sf_deposit_grid& d = grids[g];
+        if ((rc = sort_from_keys(ctx, gk.keys[g], gk.counts[g], x_m, y_m, d.val_m, nm, d.x_grid_min, d.y_grid_min, dx,
+                                 dy, d.nx, d.ny, s)))
+            return rc;
+        // as after one call per grid in order: the sum arrays hold the last grid's sums
+        const bool last = g == n_grids - 1;
+        if (wt_sum && last) {
+            SF_CUDA(cudaMemsetAsync(wt_sum, 0, (size_t)n_sum * 8, s));
+            SF_CUDA(cudaMemsetAsync(val_wt_sum, 0, (size_t)n_sum * 8, s));
+        }
+        launch_gather(ctx, d.nx, d.ny, d.val_grid, last ? val_wt_sum : nullptr, last ? wt_sum : nullptr, ld_sum, s);
+        SF_LAUNCHED(ctx);
+    }
     return SF_OK;
 }
 

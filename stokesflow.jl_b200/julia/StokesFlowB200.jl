@@ -17,7 +17,7 @@ module StokesFlowB200
 
 using CUDA
 
-export bilinearMarkerToGrid!, solveStokes!, moveMarkersRK4!, solveStokesMixed!
+export bilinearMarkerToGrid!, bilinearMarkerToGrids!, solveStokes!, moveMarkersRK4!, solveStokesMixed!
 
 const libsf = joinpath(@__DIR__, "..", "lib", "libstokesflow_b200.so")
 
@@ -68,6 +68,30 @@ function bilinearMarkerToGrid!(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m
                  Int64, Cdouble, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Int64, Int64, Ptr{Cvoid}),
                 ctx(), x_grid_min, y_grid_min, dptr(val_grid), Nx, Ny, dptr(x_m), dptr(y_m), dptr(val_m), Nm, dx, dy,
                 dptr(val_wt_sum), dptr(wt_sum), size(wt_sum, 1), length(wt_sum), stream()))
+    return nothing
+end
+
+# one grid of bilinearMarkerToGrids!: sf_deposit_grid
+struct DepositGrid
+    x_grid_min::Float64; y_grid_min::Float64
+    val_grid::Ptr{Cdouble}
+    nx::Int64; ny::Int64
+    val_m::Ptr{Cdouble}
+end
+
+# The deposits of one timestep (StokesFlow2D_multixpu.jl:164-166) in one call: grids is a list of
+# (x_grid_min, y_grid_min, val_grid, val_m); same result as bilinearMarkerToGrid! once per grid in order.
+function bilinearMarkerToGrids!(grids, x_m, y_m, dx, dy, val_wt_sum, wt_sum)
+    Nm = size(x_m, 1)
+    @assert size(y_m, 1) == Nm && all(size(g[4], 1) == Nm for g in grids)
+    GC.@preserve grids begin
+        gs = [DepositGrid(g[1], g[2], dptr(g[3]), size(g[3], 1), size(g[3], 2), dptr(g[4])) for g in grids]
+        check(ccall((:sf_bilinear_marker_to_grids, libsf), Cint,
+                    (Ptr{Cvoid}, Ptr{DepositGrid}, Cint, Ptr{Cdouble}, Ptr{Cdouble}, Int64, Cdouble, Cdouble,
+                     Ptr{Cdouble}, Ptr{Cdouble}, Int64, Int64, Ptr{Cvoid}),
+                    ctx(), gs, length(gs), dptr(x_m), dptr(y_m), Nm, dx, dy, dptr(val_wt_sum), dptr(wt_sum),
+                    size(wt_sum, 1), length(wt_sum), stream()))
+    end
     return nothing
 end
 

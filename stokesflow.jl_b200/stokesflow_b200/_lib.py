@@ -100,6 +100,12 @@ class EngineStats(C.Structure):
         return d
 
 
+class DepositGrid(C.Structure):
+    """sf_deposit_grid."""
+    _fields_ = [("x_grid_min", _d), ("y_grid_min", _d), ("val_grid", _vp), ("nx", _i64), ("ny", _i64),
+                ("val_m", _vp)]
+
+
 class Domain(C.Structure):
     """sf_domain."""
     _fields_ = [(n, _vp) for n in ("ctx", "P", "Vx_pad", "Vy_pad", "rho_vy", "mu_b", "mu_p", "dVxdt", "dVydt",
@@ -137,6 +143,8 @@ PROTOTYPES = {
     "sf_bilinear_marker_to_grid": (C.c_int, [_vp, _d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _pd, _pd,
                                              _i64, _i64, _vp]),
     "sf_bilinear_marker_to_grid_noalloc": (C.c_int, [_d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _vp]),
+    "sf_bilinear_marker_to_grids": (C.c_int, [_vp, C.POINTER(DepositGrid), C.c_int, _pd, _pd, _i64, _d, _d, _pd,
+                                              _pd, _i64, _i64, _vp]),
     "sf_solve_stokes": (C.c_int, [_vp] + [_pd] * 19 + [_d, _d, _d, _i64, _i64, _d, _d, C.c_int, _d, C.c_int, _i64,
                                                        _vp, C.POINTER(SolveInfo)]),
     "sf_stokes_residual_scale": (C.c_int, [_vp, _pd, _i64, _i64, _d, _vp, C.POINTER(_d)]),

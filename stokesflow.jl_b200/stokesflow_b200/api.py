@@ -169,6 +169,44 @@ def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, d
           "bilinear_marker_to_grid")
 
 
+def bilinear_marker_to_grids(grids, x_m, y_m, dx, dy, val_wt_sum=None, wt_sum=None, *, ctx: Context | None = None,
+                             stream=None):
+    """The deposits of one timestep in one call: ``grids`` is a sequence of (x_grid_min, y_grid_min, val_grid,
+    val_m), at most SF_MAX_GRIDS (4), over the same markers.  Same result, bit for bit, as
+    :func:`bilinear_marker_to_grid` once per grid in order (val_wt_sum / wt_sum, when given, end with the last
+    grid's sums); the markers' positions are read once for all grids' cell assignments."""
+    grids = list(grids)
+    if not 1 <= len(grids) <= 4:
+        raise ValueError("1 to 4 grids")
+    nm = x_m.numel()
+    px, py = _vec(x_m, "x_m"), _vec(y_m, "y_m")
+    if y_m.numel() != nm:
+        raise ValueError("x_m, y_m, val_m must have the same length")  # MarkerToGrid.jl:22
+    arr = (_lib.DepositGrid * len(grids))()
+    tensors = [x_m, y_m]
+    for k, (x0, y0, val_grid, val_m) in enumerate(grids):
+        if val_m.numel() != nm:
+            raise ValueError("x_m, y_m, val_m must have the same length")
+        nx, ny = val_grid.shape
+        arr[k] = _lib.DepositGrid(float(x0), float(y0), _grid(val_grid, f"grids[{k}].val_grid"), nx, ny,
+                                  _vec(val_m, f"grids[{k}].val_m"))
+        tensors += [val_grid, val_m]
+    if (val_wt_sum is None) != (wt_sum is None):
+        raise ValueError("give both val_wt_sum and wt_sum or neither")
+    ps = pw = None
+    ld = n_sum = 0
+    if wt_sum is not None:
+        ps = _grid(val_wt_sum, "val_wt_sum")
+        pw = _grid(wt_sum, "wt_sum", val_wt_sum.shape)
+        ld, n_sum = wt_sum.shape[0], wt_sum.numel()
+        tensors += [val_wt_sum, wt_sum]
+    dev = _one_device(*tensors)
+    c = _ctx_on(ctx, dev)
+    st = stream if stream is not None else torch.cuda.current_stream(dev)
+    check(lib().sf_bilinear_marker_to_grids(c.handle, arr, len(grids), px, py, nm, float(dx), float(dy), ps, pw, ld,
+                                            n_sum, _stream(st)), "bilinear_marker_to_grids")
+
+
 def bilinear_marker_to_grid_noalloc(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, dx, dy, *, stream=None):
     """The deposit of :func:`bilinear_marker_to_grid` without any device allocation, for callers that
     cannot let a library allocate GPU memory (a runtime that owns the memory through its own pool, a

@@ -141,13 +141,12 @@ class StokesFlow2D:
 
     # ------------------------------------------------------------------
     def deposit(self):
-        o, c = self.o, self.ctx
-        api.bilinear_marker_to_grid(o["x_rho"], o["y_rho"], self.rho_vy, self.x_m, self.y_m, self.rho_m, self.dx,
-                                    self.dy, self.val_wt_sum, self.wt_sum, ctx=c)
-        api.bilinear_marker_to_grid(o["x"], o["y"], self.mu_b, self.x_m, self.y_m, self.mu_m, self.dx, self.dy,
-                                    self.val_wt_sum, self.wt_sum, ctx=c)
-        api.bilinear_marker_to_grid(o["x_p"], o["y_p"], self.mu_p, self.x_m, self.y_m, self.mu_m, self.dx, self.dy,
-                                    self.val_wt_sum, self.wt_sum, ctx=c)
+        # StokesFlow2D_multixpu.jl:164-166, the three bilinearMarkerToGrid! calls in one: rho_vy, mu_b, mu_p
+        o = self.o
+        api.bilinear_marker_to_grids([(o["x_rho"], o["y_rho"], self.rho_vy, self.rho_m),
+                                      (o["x"], o["y"], self.mu_b, self.mu_m),
+                                      (o["x_p"], o["y_p"], self.mu_p, self.mu_m)],
+                                     self.x_m, self.y_m, self.dx, self.dy, self.val_wt_sum, self.wt_sum, ctx=self.ctx)
 
     def eps(self):
         if self.stokes_rtol is None:

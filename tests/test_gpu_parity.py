@@ -141,6 +141,67 @@ def test_deposit_marker_orders(sf, oracle_lib, order):
         assert np.array_equal(host(got), ref), (order, shape)
 
 
+@pytest.mark.parametrize("ngrids", [1, 3, 4])
+def test_deposit_grids_equals_one_call_per_grid(sf, oracle_lib, ngrids):
+    """The fused deposit of a timestep's grids equals one bilinear_marker_to_grid call per grid in order, bit
+    for bit: every grid, the sum arrays (the last grid's sums), and the warning counters; and the oracle."""
+    O = oracle_lib
+    Nx, Ny = 33, 27
+    dx, dy = 1.0 / (Nx - 1), 0.9 / (Ny - 1)
+    o = O.node_origins(dx, dy)
+    rng = np.random.default_rng(31)
+    nm = 20 * (Nx - 1) * (Ny - 1)
+    x = rng.random(nm) * (Nx - 1) * dx
+    y = rng.random(nm) * (Ny - 1) * dy
+    x[:4] = [-1.0, 5.0, np.nan, 2.0]
+    y[100:102] = [-3.0, np.inf]
+    vals = [np.exp(rng.normal(size=nm)) for _ in range(4)]
+    specs = [(o["x_rho"], o["y_rho"], (Nx + 1, Ny), 0), (o["x"], o["y"], (Nx, Ny), 1),
+             (o["x_p"], o["y_p"], (Nx - 1, Ny - 1), 1), (o["x_vx"], o["y_vx"], (Nx + 1, Ny - 1), 2)][:ngrids]
+    xt, yt = dev(x), dev(y)
+    vt = [dev(v) for v in vals]
+    starts = [np.asfortranarray(rng.random(shape)) for _, _, shape, _ in specs]
+    # one call per grid
+    one = [dev(a) for a in starts]
+    vws1, ws1 = sf.zeros(Nx + 1, Ny), sf.zeros(Nx + 1, Ny)
+    sf.get_warnings(reset=True)
+    for (x0, y0, _, vi), g in zip(specs, one):
+        sf.bilinear_marker_to_grid(x0, y0, g, xt, yt, vt[vi], dx, dy, vws1, ws1)
+    w1 = sf.get_warnings(reset=True)
+    # fused
+    fused = [dev(a) for a in starts]
+    vws2 = dev(np.full((Nx + 1, Ny), 7.0, order="F"))
+    ws2 = dev(np.full((Nx + 1, Ny), 7.0, order="F"))
+    sf.bilinear_marker_to_grids([(x0, y0, g, vt[vi]) for (x0, y0, _, vi), g in zip(specs, fused)], xt, yt, dx, dy,
+                                vws2, ws2)
+    w2 = sf.get_warnings(reset=True)
+    for a, b in zip(one, fused):
+        assert torch.equal(a, b)
+    assert torch.equal(vws1, vws2) and torch.equal(ws1, ws2)
+    assert w1["bad_markers"] == w2["bad_markers"] > 0 and w1["empty_nodes"] == w2["empty_nodes"]
+    for (x0, y0, shape, vi), a, g in zip(specs, starts, fused):
+        ref = a.copy(order="F")
+        O.bilinear_marker_to_grid(x0, y0, ref, x, y, vals[vi], dx, dy, F(Nx + 1, Ny), F(Nx + 1, Ny))
+        assert np.array_equal(host(g), ref)
+
+
+def test_deposit_grids_arguments(sf):
+    g = sf.zeros(6, 5)
+    x = torch.zeros(10, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError):
+        sf.bilinear_marker_to_grids([], x, x, 0.1, 0.1)
+    with pytest.raises(ValueError):
+        sf.bilinear_marker_to_grids([(0.0, 0.0, g, x)] * 5, x, x, 0.1, 0.1)
+    with pytest.raises(ValueError):
+        sf.bilinear_marker_to_grids([(0.0, 0.0, g, x[:5])], x, x, 0.1, 0.1)
+    empty = torch.empty(0, dtype=torch.float64, device="cuda")
+    val = dev(np.full((5, 4), 3.0, order="F"))
+    sf.get_warnings(reset=True)
+    sf.bilinear_marker_to_grids([(0.0, 0.0, val, empty), (0.05, 0.05, val, empty)], empty, empty, 0.1, 0.1)
+    assert np.all(host(val) == 3.0)
+    assert sf.get_warnings(reset=True)["empty_nodes"] == 40
+
+
 def test_deposit_and_rebin_with_markers_piled_in_one_cell(sf, oracle_lib):
     """Markers piled into single cells, as markers clamped into a corner pile up: one cell holds 10^5 markers
     (more than a shared-memory window of the segment sort), another 2000, the rest of the grid ~25 per cell,

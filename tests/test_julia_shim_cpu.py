@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "stokesflow_b200.h")
 SHIM = os.path.join(ROOT, "stokesflow.jl_b200", "julia", "StokesFlowB200.jl")
 
-JULIA_STRUCT_OF = {"sf_solve_info": "SolveInfo", "sf_batch_instance": "BatchInstance"}
+JULIA_STRUCT_OF = {"sf_solve_info": "SolveInfo", "sf_batch_instance": "BatchInstance", "sf_deposit_grid": "DepositGrid"}
 
 
 def _strip_c_comments(text):
@@ -128,7 +128,7 @@ def c_param_kind(p):
     simple = {"double": "Cdouble", "int64_t": "Int64", "int": "Cint", "int32_t": "Int32",
               "double*": "Ptr{Cdouble}", "constdouble*": "Ptr{Cdouble}", "void*": "Ptr{Cvoid}",
               "sf_ctx*": "Ptr{Cvoid}", "constsf_mixed_options*": "Ptr{Cvoid}", "sf_ctx**": "Ref{Ptr{Cvoid}}",
-              "constchar*": "Cstring"}
+              "constchar*": "Cstring", "constsf_deposit_grid*": "Ptr{DepositGrid}"}
     if typ in simple:
         return simple[typ]
     for cname, jname in JULIA_STRUCT_OF.items():
