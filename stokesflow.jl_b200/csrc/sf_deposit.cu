@@ -420,12 +420,9 @@ __global__ void __launch_bounds__(GT_X * GT_Y, 8) k_gather_sorted(const Payload*
         atomicAdd(empty_counter, 1ull);
 }
 
-// The allocation-free deposit's gather (its scratch holds no payload): the same merge, reading each marker's
-// position and value through the sorted permutation.
-// 5. per-node gather.  Node (I, J), 1-based.  A marker in cell (ix, iy)
-// contributes to node (ix, iy) with (1-dx)(1-dy), (ix+1, iy) with dx(1-dy),
-// (ix, iy+1) with (1-dx)dy and (ix+1, iy+1) with dx*dy (MarkerToGrid.jl:124-151),
-// so node (I, J) merges the cells (I,J), (I-1,J), (I,J-1), (I-1,J-1).
+// The allocation-free deposit's gather (its scratch holds no payload): the same merge of node (I, J)'s cells
+// (I,J), (I-1,J), (I,J-1), (I-1,J-1) in ascending marker index, reading each marker's position and value
+// through the sorted permutation.
 __global__ void k_gather(const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ val,
                          const int32_t* __restrict__ offsets, const int32_t* __restrict__ perm, int64_t nx,
                          int64_t ny, double xmin, double ymin, double dx, double dy, double* __restrict__ val_grid,
