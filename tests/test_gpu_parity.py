@@ -185,6 +185,31 @@ def test_deposit_grids_equals_one_call_per_grid(sf, oracle_lib, ngrids):
         assert np.array_equal(host(g), ref)
 
 
+def test_deposit_grids_with_markers_piled_in_cells(sf, oracle_lib):
+    """The fused deposit with cells holding 3*10^4 and 2000 markers (each grid's long-cell radix sort works in
+    that grid's own slice of the key buffer), against the oracle on all three staggered grids."""
+    O = oracle_lib
+    Nx, Ny = 30, 24
+    dx, dy = 0.04, 0.05
+    rng = np.random.default_rng(41)
+    n0, n1, n2 = 20_000, 30_000, 2_000
+    x = np.concatenate([rng.random(n0) * (Nx - 1) * dx, (5 + rng.random(n1)) * dx, (20 + rng.random(n2)) * dx])
+    y = np.concatenate([rng.random(n0) * (Ny - 1) * dy, (7 + rng.random(n1)) * dy, (15 + rng.random(n2)) * dy])
+    order = rng.permutation(x.size)
+    x, y = x[order], y[order]
+    rho, mu = np.exp(rng.normal(size=x.size)), np.exp(rng.normal(size=x.size))
+    o = O.node_origins(dx, dy)
+    specs = [(o["x_rho"], o["y_rho"], (Nx + 1, Ny), rho), (o["x"], o["y"], (Nx, Ny), mu),
+             (o["x_p"], o["y_p"], (Nx - 1, Ny - 1), mu)]
+    grids = [sf.zeros(*shape) for _, _, shape, _ in specs]
+    sf.bilinear_marker_to_grids([(x0, y0, g, dev(v)) for (x0, y0, _, v), g in zip(specs, grids)], dev(x), dev(y),
+                                dx, dy)
+    for (x0, y0, shape, v), g in zip(specs, grids):
+        ref = F(*shape)
+        O.bilinear_marker_to_grid(x0, y0, ref, x, y, v, dx, dy, F(Nx + 1, Ny), F(Nx + 1, Ny))
+        assert np.array_equal(host(g), ref), shape
+
+
 def test_deposit_grids_arguments(sf):
     g = sf.zeros(6, 5)
     x = torch.zeros(10, dtype=torch.float64, device="cuda")
