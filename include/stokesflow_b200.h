@@ -70,6 +70,13 @@ typedef struct {
 } sf_warnings;
 int sf_get_warnings(sf_ctx* ctx, sf_warnings* out, int reset);
 
+/* Self-test of the bounded waits that every persistent kernel uses (a wall-clock budget on an mbarrier, then an
+ * error flag instead of a hang).  One block waits on a shared-memory barrier for at most budget_ns
+ * (1 .. 2e9): with arrive != 0 the barrier is completed first and *timed_out is 0; with arrive == 0 nothing
+ * completes it, every thread gives up after the budget and *timed_out is 1.  Either way the kernel returns
+ * and the context stays usable.  Synchronises the context's work stream. */
+int sf_selftest_bounded_wait(sf_ctx* ctx, int arrive, int64_t budget_ns, int32_t* timed_out);
+
 /* ---------------------------------------------------------------------- */
 /* marker->grid deposit                                                     */
 /* ---------------------------------------------------------------------- */

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "sf_internal.cuh"
+#include "sf_tma.cuh"
 
 namespace sf {
 
@@ -318,6 +319,21 @@ __global__ void k_set_props(sf_plume_model M, const double* __restrict__ x, cons
     }
 }
 
+// The bounded wait of the persistent kernels (mbar_wait), on a shared-memory barrier that thread 0 completes
+// (arrive != 0) or that nothing completes (arrive == 0): then every thread's wait gives up after budget_ns and
+// the block reports it through *timed_out, exactly as the kernels report a tile copy that never landed.
+__global__ void k_wait_selftest(int arrive, uint64_t budget_ns, int* __restrict__ timed_out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (arrive && threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 0);
+    const bool ok = mbar_wait(&bar, 0, budget_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicExch(timed_out, 1);
+}
+
 }  // namespace sf
 
 using namespace sf;
@@ -429,6 +445,21 @@ int sf_get_warnings(sf_ctx* c, sf_warnings* out, int reset) {
     out->interp_failsafe = (int64_t)h[CNT_INTERP_FAILSAFE];
     out->markers_outside = (int64_t)h[CNT_OUTSIDE];
     if (reset) SF_CUDA(cudaMemset(c->d_counters, 0, sizeof(h)));
+    return SF_OK;
+}
+
+int sf_selftest_bounded_wait(sf_ctx* c, int arrive, int64_t budget_ns, int32_t* timed_out) {
+    if (!c || !timed_out) return fail(SF_ERR_INVALID_ARG, "sf_selftest_bounded_wait: NULL argument");
+    if (budget_ns < 1 || budget_ns > 2000000000LL)
+        return fail(SF_ERR_INVALID_ARG, "sf_selftest_bounded_wait: budget_ns must be in 1 .. 2e9");
+    int rc = set_device(c);
+    if (rc) return rc;
+    int* d = c->d_flags + 1;   // the second flag word: the solvers' copy-timeout flag stays untouched
+    SF_CUDA(cudaMemsetAsync(d, 0, sizeof(int), c->work));
+    k_wait_selftest<<<1, 128, 0, c->work>>>(arrive, (uint64_t)budget_ns, d);
+    SF_LAUNCHED(c);
+    SF_CUDA(cudaMemcpyAsync(timed_out, d, sizeof(int), cudaMemcpyDeviceToHost, c->work));
+    SF_CUDA(cudaStreamSynchronize(c->work));
     return SF_OK;
 }
 

@@ -11,8 +11,8 @@ from ._lib import LIB_PATH, StokesFlowError, build, lib  # noqa: F401
 from .api import (Context, Engine, MixedProblem, PlumeModel, batch_stats, bilinear_marker_to_grid,  # noqa: F401
                   bilinear_marker_to_grid_noalloc, bilinear_marker_to_grids, default_context, get_warnings,
                   initialize_markers, initialize_markers_host, marker_count, mixed_options, move_markers_rk4, rebin_markers,
-                  residual_scale, set_initial_marker_properties, solve_stokes, solve_stokes_batch_mixed,
-                  solve_stokes_info, zeros)
+                  residual_scale, selftest_bounded_wait, set_initial_marker_properties, solve_stokes,
+                  solve_stokes_batch_mixed, solve_stokes_info, zeros)
 from .driver import (StokesFlow2D, node_origins, plume_model_test_flow, plume_model_unit_square,  # noqa: F401
                      stokes_flow_2d)
 

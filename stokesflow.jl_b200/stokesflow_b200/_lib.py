@@ -140,6 +140,7 @@ PROTOTYPES = {
     "sf_ctx_scratch_bytes": (C.c_int, [_vp, C.POINTER(_i64)]),
     "sf_ctx_launch_count": (C.c_int, [_vp, C.POINTER(_i64)]),
     "sf_get_warnings": (C.c_int, [_vp, C.POINTER(Warnings), C.c_int]),
+    "sf_selftest_bounded_wait": (C.c_int, [_vp, C.c_int, _i64, C.POINTER(_i32)]),
     "sf_bilinear_marker_to_grid": (C.c_int, [_vp, _d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _pd, _pd,
                                              _i64, _i64, _vp]),
     "sf_bilinear_marker_to_grid_noalloc": (C.c_int, [_d, _d, _pd, _i64, _i64, _pd, _pd, _pd, _i64, _d, _d, _vp]),

@@ -144,6 +144,15 @@ def _ctx_on(ctx: Context | None, device: torch.device) -> Context:
 
 
 # ---------------------------------------------------------------------------
+def selftest_bounded_wait(arrive: bool, budget_ns: int, *, ctx: Context | None = None) -> bool:
+    """Runs the kernels' bounded wait on a barrier that is completed first (arrive) or that nothing completes;
+    returns True if the wait gave up after budget_ns.  The context stays usable either way."""
+    out = C.c_int32(0)
+    check(lib().sf_selftest_bounded_wait(_ctx(ctx).handle, int(bool(arrive)), int(budget_ns), C.byref(out)),
+          "selftest_bounded_wait")
+    return bool(out.value)
+
+
 def bilinear_marker_to_grid(x_grid_min, y_grid_min, val_grid, x_m, y_m, val_m, dx, dy, val_wt_sum=None,
                             wt_sum=None, grid=None, *, ctx: Context | None = None, stream=None):
     """bilinearMarkerToGrid! (MarkerToGrid.jl:18-38): deposit val_m onto val_grid in place."""
