@@ -790,7 +790,8 @@ def _brief(d, keys):
 def run_forms(a):
     """The three further forms, bounded so that they add a few minutes to the default run: a batch of
     forms_batch instances of the batching workload with the full plain FP64 loop over the same instances, a
-    serve trace of forms_requests requests, and one precision case of forms_precision_n^2 grid points."""
+    serve trace of forms_requests requests (against the plain FP64 server one request at a time and with
+    fp64_concurrency workers), and one precision case of forms_precision_n^2 grid points."""
     forms = {}
     t0 = time.perf_counter()
     b = run_batch_form(a, instances=a.forms_batch, cells=a.batch_cells, concurrency=1)
@@ -798,10 +799,14 @@ def run_forms(a):
                                 "p99_latency_s", "fp64_loop_p50_latency_s", "fp64_loop_p99_latency_s", "max_rel_l2",
                                 "median_rel_l2", "same_iterations", "compared", "instances", "converged",
                                 "fp64_converged", "clocks", "config"))
-    s = run_serve_form(a, requests=a.forms_requests, rate=a.forms_rate, cells=a.forms_cells, concurrency=1)
+    # the plain FP64 server both one request at a time (the plain form as it is called) and with
+    # fp64_concurrency workers, so that the batching gain and the precision gain can be told apart
+    s = run_serve_form(a, requests=a.forms_requests, rate=a.forms_rate, cells=a.forms_cells,
+                       concurrency=a.fp64_concurrency)
     forms["serve"] = _brief(s, ("solves_per_s", "p50_latency_s", "p99_latency_s", "fp64_solves_per_s",
-                                "fp64_p50_latency_s", "fp64_p99_latency_s", "speedup_solves_per_s", "max_rel_l2",
-                                "median_rel_l2", "compared_requests", "clocks", "config"))
+                                "fp64_p50_latency_s", "fp64_p99_latency_s", "speedup_solves_per_s",
+                                "fp64_concurrent", "speedup_vs_fp64_concurrent", "max_rel_l2", "median_rel_l2",
+                                "compared_requests", "clocks", "config"))
     forms["serve"]["requests"] = s["mixed"]["requests"]
     forms["serve"]["solves"] = s["mixed"]["solves"]
     p = run_precision_form(a, n=a.forms_precision_n, cases=1, steps=a.forms_precision_steps,
