@@ -506,8 +506,12 @@ def run_precision_form(a, *, n=None, cases=None, steps=None, contrast=None):
         model = sf.plume_model_unit_square()
         model.mu_air = a.mu_air
         model.mu_plume = model.mu_matrix / C
+        # the mixed path on a context of its own: its sweep tuner measures this workload instead of reusing a
+        # choice recorded for another form's instances in the same workload class
+        mctx = sf.Context(0)
         states = {s: sf.StokesFlow2D(n, n, 1.0, 1.0, model, marker_density=md, stokes_rtol=a.rtol, jitter=0.5,
-                                     seed=0, iter_max=SOLVE_CAP, keep_work_arrays=False, solver=s, mixed_opts=opts)
+                                     seed=0, iter_max=SOLVE_CAP, keep_work_arrays=False, solver=s, mixed_opts=opts,
+                                     ctx=mctx if s == "mixed" else None)
                   for s in ("fp64", "mixed")}
         rows = []
         for k in range(steps):
@@ -522,10 +526,15 @@ def run_precision_form(a, *, n=None, cases=None, steps=None, contrast=None):
                          "rel_l2_markers_y": _rel_l2(m.y_m, f.y_m)})
         fs = sum(r["fp64_solve_ms"] for r in rows)
         ms = sum(r["mixed_solve_ms"] for r in rows)
+        eng = sf.batch_stats(mctx)
         out_cases.append({"contrast": C, "mu_plume": model.mu_plume, "fp64_solve_ms_total": round(fs, 1),
                           "mixed_solve_ms_total": round(ms, 1), "solve_speedup": round(fs / ms, 3),
-                          "same_iterations": all(r["fp64_iters"] == r["mixed_sweeps"] for r in rows), "steps": rows})
+                          "same_iterations": all(r["fp64_iters"] == r["mixed_sweeps"] for r in rows),
+                          "sweeps": {k: eng.get(k) for k in ("tile_rows", "tile_schedule", "overlap_launches",
+                                                             "tune_state")},
+                          "steps": rows})
         del states
+        mctx.close()
         torch.cuda.empty_cache()
     clk = clocks.stop()
     fs = sum(cs["fp64_solve_ms_total"] for cs in out_cases)
@@ -814,6 +823,7 @@ def run_forms(a):
     forms["precision"] = _brief(p, ("solves_per_s", "fp64_solves_per_s", "solve_speedup", "max_rel_l2",
                                     "same_iterations", "clocks", "config"))
     forms["precision"]["iterations"] = [[r["fp64_iters"], r["mixed_sweeps"]] for r in p["cases"][0]["steps"]]
+    forms["precision"]["sweeps"] = p["cases"][0]["sweeps"]
     forms["wall_s"] = round(time.perf_counter() - t0, 1)
     forms["bar"] = {"rel_l2": 1e-5, "speedup_solves_per_s": 1.8,
                     "note": "rel L2 of the FP32-with-correction result against the plain FP64 path (the oracle) at "
