@@ -72,11 +72,15 @@ def parse():
     ap.add_argument("--pt32-probe", type=int, default=0, metavar="SWEEPS",
                     help="kernel probe: one n x n instance through the mixed engine for exactly SWEEPS FP32 sweeps "
                          "(one fold); prints the sweep time; used for ncu captures of k_pt32")
-    ap.add_argument("--form", default="timestep", choices=["timestep", "precision", "batch", "serve", "tune"],
+    ap.add_argument("--form", default="timestep",
+                    choices=["timestep", "precision", "batch", "serve", "tune", "decomposed"],
                     help="timestep: the plain FP64 timestep (default line); precision: the same timesteps with FP32 "
                          "sweeps + FP64 correction beside the plain path; batch: many independent solves in one "
                          "engine vs a loop of plain FP64 solves; serve: a Poisson request stream, continuous "
-                         "batching vs plain FP64 serving; tune: the sweep tuner's table of tile shapes and schedules")
+                         "batching vs plain FP64 serving; tune: the sweep tuner's table of tile shapes and schedules; "
+                         "decomposed: the PT solve over a grid of ranks vs the single-domain solve of the same grid")
+    ap.add_argument("--dims", default="2,2", help="decomposed form: ranks in x and y")
+    ap.add_argument("--decomposed-iters", type=int, default=2000, help="decomposed form: PT iterations timed")
     ap.add_argument("--precision-cases", type=int, default=2, help="precision form: plume contrasts drawn from seed")
     ap.add_argument("--precision-contrast", default="0,2",
                     help="precision form: log10 range of matrix/plume viscosity, log-uniform (soft plume)")
@@ -165,6 +169,55 @@ def pt32_probe(a):
     print(json.dumps({"probe": "k_pt32", "n": n, "sweeps": r["inner_iters"], "us_per_sweep": round(us, 3),
                       "gpts_per_s": round(pts / us / 1e3, 2), "t_eff_gbs": round(gbs, 1),
                       "frac_of_peak": round(gbs / peak, 4), "peak_source": src}), flush=True)
+
+
+def run_decomposed_form(a):
+    """The decomposed PT solve (sf_solve_stokes_decomposed: a grid of ranks with halo updates and the global
+    reductions) on the ranks' devices -- here all on this GPU -- against the single-domain solve of the same
+    global grid: the same plume fields, split as the ranks hold them, iterated a fixed number of times from rest
+    (no residual small enough to stop them).  Reports microseconds per PT iteration of each; the decomposed solve
+    issues its launches and halo copies from the host, rank by rank, every iteration."""
+    import stokesflow_b200 as sf
+    from stokesflow_b200 import domains
+    torch.cuda.set_device(0)
+    dims = _pair(a.dims, int)
+    n = a.n
+    nloc = domains.local_size(dims[0], n), domains.local_size(dims[1], n)
+    iters = a.decomposed_iters
+    model = sf.plume_model_unit_square()
+    model.mu_air = a.mu_air
+    md = sf.driver.marker_density_for(a.markers_per_cell)
+    st = sf.StokesFlow2D(n, n, 1.0, 1.0, model, marker_density=md, stokes_rtol=a.rtol, jitter=0.5, seed=0,
+                         iter_max=iters, keep_work_arrays=False)
+    st.deposit()
+    names = ("P", "Vx_pad", "Vy_pad", "rho_vy", "mu_b", "mu_p", "dVxdt", "dVydt", "Vx_s", "Vy_s")
+    glob = {"P": st.P, "Vx_pad": st.Vx, "Vy_pad": st.Vy, "rho_vy": st.rho_vy, "mu_b": st.mu_b, "mu_p": st.mu_p,
+            "dVxdt": st.dVxdt, "dVydt": st.dVydt, "Vx_s": st.Vx_s, "Vy_s": st.Vy_s}
+    ranks = domains.split({k: glob[k] for k in names}, dims, nloc[0], nloc[1])
+    ctxs = {c: sf.Context(0) for c in ranks}
+    out = {}
+    for rep in range(2):   # the first of each is a warm-up
+        t = {}
+        info = sf.solve_stokes_info(st.P, st.Vx, st.Vy, st.rho_vy, st.mu_b, st.mu_p, None, None, None, None, None,
+                                    None, None, st.dVxdt, st.dVydt, None, None, st.Vx_s, st.Vy_s, st.g_y, st.dx,
+                                    st.dy, n, n, 0.0, st.maxdisp, eps=1e-300, iter_max=iters, ctx=st.ctx)
+        t["single"] = (info["loop_ms"], info["iters"])
+        loc = {c: {k: v.clone() for k, v in r.items()} for c, r in ranks.items()}
+        d = domains.solve_stokes_decomposed(loc, dims, nloc[0], nloc[1], st.g_y, st.dx, st.dy, 0.0, st.maxdisp,
+                                            eps=1e-300, iter_max=iters, contexts=ctxs)
+        t["decomposed"] = (d["loop_ms"], d["iters"])
+        out = t
+    us = {k: v[0] * 1e3 / max(1, v[1]) for k, v in out.items()}
+    for c in ctxs.values():
+        c.close()
+    return {"form": "decomposed", "metric": "microseconds per PT iteration, FP64", "unit": "us",
+            "us_per_iter_single_domain": round(us["single"], 2), "us_per_iter_decomposed": round(us["decomposed"], 2),
+            "decomposed_over_single": round(us["decomposed"] / us["single"], 3),
+            "iterations": {k: v[1] for k, v in out.items()},
+            "config": {"workload": f"plume, {n}x{n} grid points, fields deposited from {md * md} markers per cell; "
+                                   f"{dims[0]}x{dims[1]} ranks of {nloc[0]}x{nloc[1]} points, all on one GPU",
+                       "note": "single-domain time from the library's CUDA events over the PT loop; decomposed time "
+                               "from its host clock over the loop (launches and halo copies issued rank by rank)"}}
 
 
 def run_tune_form(a):
@@ -878,7 +931,7 @@ def main():
     if a.form != "timestep" and a.impl == "ours":
         if rank == 0:
             run = {"precision": run_precision_form, "batch": run_batch_form, "serve": run_serve_form,
-                   "tune": run_tune_form}[a.form]
+                   "tune": run_tune_form, "decomposed": run_decomposed_form}[a.form]
             print(json.dumps(run(a)), flush=True)
         return
     if a.impl == "reference":
