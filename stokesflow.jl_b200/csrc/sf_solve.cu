@@ -953,6 +953,59 @@ static int global_dt(std::vector<Rank>& R, double maxdisp, double dx, double dy,
     return SF_OK;
 }
 
+// Two plain PT iterations of every rank (kernels, their events, the halo updates), captured from the ranks'
+// streams into one graph.  Only for ranks that share a device.  The graph starts with every rank's first
+// kernel (the launch waits for all earlier work); the second iteration waits on the neighbours' events as the
+// direct loop does.  The host-side buffer parity flips twice, so it ends where it started and the graph belongs
+// to that parity.  *launches_out: the kernels the graph holds, per rank.  On any failure the capture is ended,
+// the parity restored and a status returned: the caller then keeps launching directly.
+static int capture_two_iterations(std::vector<Rank>& R, int64_t Nx, int64_t Ny, cudaEvent_t fork,
+                                  std::vector<cudaEvent_t>& joins, cudaGraphExec_t* out,
+                                  std::vector<int64_t>& launches_out) {
+    std::vector<int> parity(R.size());
+    std::vector<int64_t> l0(R.size());
+    for (size_t k = 0; k < R.size(); ++k) {
+        parity[k] = R[k].S.cur;
+        l0[k] = R[k].ctx->launches;
+    }
+    cudaStream_t s0 = R[0].s;
+    SF_CUDA(cudaSetDevice(R[0].ctx->device));
+    SF_CUDA(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+    int rc = SF_OK;
+    cudaError_t e = cudaEventRecord(fork, s0);
+    for (size_t k = 1; k < R.size() && e == cudaSuccess; ++k) e = cudaStreamWaitEvent(R[k].s, fork, 0);
+    for (int it = 0; it < 2 && rc == SF_OK && e == cudaSuccess; ++it) {
+        if (it == 1)
+            for (Rank& k : R)
+                for (int n : {k.left, k.right, k.down, k.up})
+                    if (n >= 0 && e == cudaSuccess) e = cudaStreamWaitEvent(k.s, R[n].ev, 0);
+        for (Rank& k : R) {
+            if (rc == SF_OK && e == cudaSuccess) rc = k.S.launch_iter(false);
+            if (rc == SF_OK && e == cudaSuccess) e = cudaEventRecord(k.ev, k.s);
+        }
+        if (rc == SF_OK && e == cudaSuccess) rc = update_halos(R, state_halos(R), Nx, Ny);
+    }
+    for (size_t k = 1; k < R.size() && e == cudaSuccess; ++k) {
+        e = cudaEventRecord(joins[k], R[k].s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s0, joins[k], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s0, &g);
+    for (size_t k = 0; k < R.size(); ++k) {
+        R[k].S.cur = parity[k];
+        launches_out[k] = R[k].ctx->launches - l0[k];
+        R[k].ctx->launches = l0[k];
+    }
+    if (rc == SF_OK && (e != cudaSuccess || ee != cudaSuccess)) rc = fail(SF_ERR_CUDA, "decomposed solve: graph capture");
+    if (rc == SF_OK && cudaGraphInstantiate(out, g, 0) != cudaSuccess) rc = fail(SF_ERR_CUDA, "decomposed solve: graph");
+    if (g) cudaGraphDestroy(g);
+    if (rc != SF_OK) {
+        *out = nullptr;
+        (void)cudaGetLastError();
+    }
+    return rc;
+}
+
 static int set_scalar_all(std::vector<Rank>& R, int slot, double v) {
     for (Rank& k : R) {
         SF_CUDA(cudaSetDevice(k.ctx->device));
@@ -1154,10 +1207,64 @@ int sf_solve_stokes_decomposed(sf_domain* domains, int32_t dims_x, int32_t dims_
     struct Guard { std::function<void()> f; ~Guard() { f(); } } guard{destroy_events};
 
     // ---- PT loop (:43-77), every rank per iteration, halos after it (:57) ----
+    // Ranks that share a device run their plain iterations (no store, dt update or check) two at a time from a
+    // captured graph, one per buffer parity: one host launch instead of every rank's kernels, events and halo
+    // copies.  Ranks on several devices launch directly.
+    bool graphs = nr > 1;
+    for (const Rank& k : R) graphs = graphs && k.ctx->device == R[0].ctx->device;
+    cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+    std::vector<int64_t> glaunches[2] = {std::vector<int64_t>((size_t)nr, 0), std::vector<int64_t>((size_t)nr, 0)};
+    cudaEvent_t gfork = nullptr, gdone = nullptr;
+    // gjoin are recorded inside the capture only; gpre order the graph launch after every rank's earlier work
+    // (an event last recorded inside a capture cannot be waited on outside it)
+    std::vector<cudaEvent_t> gjoin((size_t)nr, nullptr), gpre((size_t)nr, nullptr);
+    auto destroy_graphs = [&]() {
+        for (cudaGraphExec_t& x : gexec)
+            if (x) cudaGraphExecDestroy(x);
+        if (gfork) cudaEventDestroy(gfork);
+        if (gdone) cudaEventDestroy(gdone);
+        for (cudaEvent_t ev : gjoin)
+            if (ev) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : gpre)
+            if (ev) cudaEventDestroy(ev);
+    };
+    struct Guard2 { std::function<void()> f; ~Guard2() { f(); } } guard2{destroy_graphs};
+    if (graphs) {
+        SF_CUDA(cudaSetDevice(R[0].ctx->device));
+        SF_CUDA(cudaEventCreateWithFlags(&gfork, cudaEventDisableTiming));
+        SF_CUDA(cudaEventCreateWithFlags(&gdone, cudaEventDisableTiming));
+        for (cudaEvent_t& ev : gjoin) SF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        for (cudaEvent_t& ev : gpre) SF_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
+    auto plain = [&](int64_t it) {
+        return it < iter_max && it % ncheck != 0 && !(use_stab && it % ndtupdate == 0);
+    };
     const auto t0 = std::chrono::steady_clock::now();
     double err = 2.0 * eps;
     int64_t iter = 1, niter = 0, nchecks = 0;
     while (err > eps && iter <= iter_max) {
+        if (graphs && plain(iter) && plain(iter + 1)) {
+            const int par = R[0].S.cur;
+            if (!gexec[par] && capture_two_iterations(R, Nx, Ny, gfork, gjoin, &gexec[par], glaunches[par]))
+                graphs = false;   // keep launching directly
+            if (gexec[par]) {
+                SF_CUDA(cudaSetDevice(R[0].ctx->device));
+                for (size_t k = 0; k < R.size(); ++k) {   // every rank's earlier work
+                    SF_CUDA(cudaEventRecord(gpre[k], R[k].s));
+                    SF_CUDA(cudaStreamWaitEvent(R[0].s, gpre[k], 0));
+                }
+                SF_CUDA(cudaGraphLaunch(gexec[par], R[0].s));
+                SF_CUDA(cudaEventRecord(gdone, R[0].s));
+                for (size_t k = 0; k < R.size(); ++k) {
+                    SF_CUDA(cudaStreamWaitEvent(R[k].s, gdone, 0));
+                    SF_CUDA(cudaEventRecord(R[k].ev, R[k].s));
+                    R[k].ctx->launches += glaunches[par][k];
+                }
+                niter += 2;
+                iter += 2;
+                continue;
+            }
+        }
         const bool store = (iter % ncheck == 0) || (iter == iter_max);
         for (Rank& k : R) {
             SF_CUDA(cudaSetDevice(k.ctx->device));
